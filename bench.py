@@ -1,0 +1,335 @@
+"""Benchmark of the fused B200 time step on the single-grid plain-FP32 workload:
+hydro scheme, 4096 x 4096 periodic Kelvin-Helmholtz shear layer (tanh profile, seeded
+noise), FP32 state, CFL time step kept on the device, 1000 RK3 steps per run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fused|reference]
+
+One process per GPU (torchrun for N > 1); the single grid does not shard, so N GPUs run N
+independent replicas and `value` is their aggregate (weak scaling).  Rank 0 prints one
+JSON line.  `--impl reference` times the reference's CPU arithmetic (oracle/_ref, the
+reference's own stencil/RHS headers compiled for the host; the CPU port where that build is
+absent) on the host cores instead, on rank 0 only.
+"""
+import argparse
+import datetime
+import glob
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N1 = N2 = 4096
+SCHEME, SETUP, SEED = "hydro", "kh", 2
+NVAR = 4
+ELEM = 4
+# Algorithmic HBM bytes per cell and stage: stage 0 reads u, writes v and u'; stage 1
+# reads u and v, writes v and u'; stage 2 reads u and v, writes u' (v is dead).
+B_STAGE = [3 * NVAR * ELEM, 4 * NVAR * ELEM, 3 * NVAR * ELEM]
+B_ALG = sum(B_STAGE)  # 160 B per cell-step
+METRIC = "Gcell-steps/s"
+WORKLOAD = "hydro 4096x4096 periodic tanh Kelvin-Helmholtz, plain FP32 fused RK3 step, device-resident CFL dt"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(key):
+    """Per-launch DRAM bytes of the substage kernel from a committed ncu summary line
+    `bench-traffic: <key> <bytes>` in profiles/*.md, or None."""
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        for line in open(p):
+            m = re.match(r"\s*bench-traffic:\s*(\S+)\s+([0-9.eE+]+)", line)
+            if m and m.group(1) == key:
+                return float(m.group(2))
+    return None
+
+
+# ---- distributed plumbing (also exercised by tests/test_bench_dist.py with gloo) ---------
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def dist_init(world, backend):
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist if world > 1 else None
+
+
+def reduce_max(x, dist, device):
+    """Max of a float over ranks (the timing rule: slowest rank)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        dist.all_reduce(t)
+
+
+def aggregate_rate(cells_per_rank, steps, world, max_seconds):
+    """Whole-job Gcell-steps/s: all ranks' cell-steps over the slowest rank's time."""
+    return world * cells_per_rank * steps / max_seconds / 1e9
+
+
+# ---- clocks --------------------------------------------------------------------------
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={CLOCK_QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+                except ValueError:
+                    continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        loaded = [r for r in rows if r[2] > 200.0] or rows  # samples under load (power draw)
+        reasons = sorted({names[k] for r in loaded for k in range(4) if r[3][k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median([r[0] for r in loaded])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(loaded), "power_w_max": max(r[2] for r in rows)}
+
+
+# ---- CPU arithmetic of the reference ------------------------------------------------------
+def cpu_sample(state, rows, steps, dt):
+    """Time `steps` RK3 steps of the reference's CPU arithmetic on a periodic 4096-wide strip
+    of `rows` rows cut from the workload's state.  Returns (Gcell-steps/s, kind, cores)."""
+    from oracle.oracle import Oracle, available, reference_delta
+    kind = "reference" if available(SCHEME, "f32", "reference") else "port"
+    o = Oracle(SCHEME, "f32", kind)
+    cores = o.threads(os.cpu_count() or 1)
+    o.set_delta(*reference_delta(N1, N2, 1.0, 1.0))
+    u = o.padded(np.ascontiguousarray(state[:rows]))
+    v = o.empty(rows, N2)
+    t0 = time.perf_counter()
+    o.run(u, v, 0.0, dt, steps)
+    el = time.perf_counter() - t0
+    return rows * N2 * steps / el / 1e9, kind, cores, el
+
+
+def calibrated_rows(state, dt, budget_s, per_steps):
+    rate, _, _, _ = cpu_sample(state, 32, 1, dt)
+    rows = int(budget_s * rate * 1e9 / (N2 * per_steps))
+    return max(16, min(N1, rows))
+
+
+def initial_state():
+    import fg2_b200
+    q, _ = fg2_b200.setup_evaluate(SETUP, N1, N2, SCHEME, seed=SEED)
+    return q.astype(np.float32)
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    state = initial_state()
+    dt = 2.0e-5  # a stable step of this workload (the CFL step at t = 0 is about 1.9e-5)
+    rows = calibrated_rows(state, dt, 120.0 / max(1, args.steps + args.warmup), 1)
+    for _ in range(args.warmup):
+        cpu_sample(state, rows, 1, dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, kind, cores, _ = cpu_sample(state, rows, 1, dt)
+    el = time.perf_counter() - t0
+    value = rows * N2 * args.steps / el / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3 * (N1 / rows),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scheme": SCHEME, "grid": [N1, N2]},
+        "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
+                         "sample": f"each step: one RK3 step on a periodic {rows}x{N2} strip of the 4096^2 state"},
+        "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ns_per_cell_step": 1.0 / value,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- the fused GPU path -------------------------------------------------------------------
+def run_fused(args):
+    import torch
+    import fg2_b200
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = dist_init(world, "nccl")
+
+    sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage="f32")
+    sim.config()
+    state = initial_state()
+    sim.upload(state)
+    sim.set_dt_mode("cfl")
+    stream = torch.cuda.ExternalStream(sim.stream, device=device)
+    cells = N1 * N2
+
+    # warm-up (graph capture happens here)
+    sim.set_time(0.0)
+    sim.advance(max(args.warmup, 3), 0.0, graph=True)
+    if sim.sync() != 0:
+        raise RuntimeError("warm-up produced a bad status")
+
+    # timed region: K steps through the graph, device-resident CFL dt
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.advance(args.steps, 0.0, graph=True)
+        ev1.record(stream)
+        ev1.synchronize()
+    status = sim.sync()
+    torch.cuda.synchronize()
+    barrier(dist, device)
+    ms = reduce_max(ev0.elapsed_time(ev1), dist, device)
+    value = aggregate_rate(cells, args.steps, world, ms / 1e3)
+    sim_time = sim.time()
+
+    # per-launch duration of the substage kernel, live, on the launching stream
+    dt_fixed = sim.last_dt()
+    reps = 20
+    evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+           for _ in range(3)]
+    for r in range(reps):
+        for k in range(3):
+            evs[k][r][0].record(stream)
+            sim.stage(k, dt_fixed)
+            evs[k][r][1].record(stream)
+    torch.cuda.synchronize()
+    stage_ms = [float(np.mean([a.elapsed_time(b) for a, b in evs[k][2:]])) for k in range(3)]
+    if sim.sync() != 0:
+        raise RuntimeError("stage timing produced a bad status")
+    peak, peak_kind = peaks()
+    achieved = B_ALG * cells / (sum(stage_ms) / 1e3) / 1e9  # GB/s over the three launches
+    traffic = profiled_traffic("substage_hydro_f32_4096")
+
+    # end to end through the public API: pinned host state in, K steps, state out
+    host = torch.empty((N1, N2, NVAR), dtype=torch.float32, pin_memory=True).numpy()
+    host[...] = state
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.upload(host)
+    sim.set_time(0.0)
+    sim.advance(args.steps, 0.0, graph=True)
+    e2e_status = sim.sync()
+    sim.download(out=host)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1), dist, device)
+    state_bytes = cells * NVAR * ELEM
+    e2e = {"value": aggregate_rate(cells, args.steps, world, e2e_ms / 1e3), "unit": "Gcell-steps/s",
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": (state_bytes + 64) / args.steps,
+           "what": "one frame through the C ABI: pinned host state uploaded, K graph-replayed steps, "
+                   "status read, state downloaded"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rows = calibrated_rows(state, 2.0e-5, 15.0, 2)
+        rate, kind, cores, el = cpu_sample(state, rows, 2, 2.0e-5)
+        cpu = {"value": rate, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
+               "sample": f"2 RK3 steps on a periodic {rows}x{N2} strip of the 4096^2 state ({el:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded tanh Kelvin-Helmholtz shear layer (setup kh, seed 2)",
+            "config": {"workload": WORKLOAD, "scheme": SCHEME, "grid": [N1, N2], "setup": SETUP, "seed": SEED,
+                       "dt": "CFL + diffusive limit, FP64, device-resident", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (u, u' and v are 268 MB each)"},
+            "ns_per_cell_step": 1.0 / (value / world),
+            "status": status, "sim_time": sim_time,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "frac_nominal_8tbs": achieved / 8000.0,
+                         "bytes_per_cell_step": B_ALG, "stage_ms": stage_ms},
+            "step_hbm_frac": value / world * B_ALG / peak,
+            "cpu_baseline": cpu,
+            "e2e": e2e, "e2e_status": e2e_status,
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_fused(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,72 @@
+// fg2_b200/csrc/kernels.h -- host-side launchers of the device kernels (kernels.cu),
+// used by the runtime (runtime.cpp).  All launches are asynchronous on `stream`.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "fg2b.h"
+
+namespace fg2 {
+
+// Scalar inputs of one substage launch (RK3 stage s: v <- F(u) + beta v,
+// u_out <- u + gamma dt v), all in the host's double precision; each launcher rounds them
+// to the compute type the way the reference rounds E-precision coefficients to R.
+struct StageArgs {
+  double beta;          // the stage's beta (src/step.cpp:25)
+  double gamma;         // the stage's gamma (src/step.cpp:26)
+  double dt;            // time step when dt_dev is null
+  const double *dt_dev; // device-resident time step (graph-captured runs), or null
+  double delta1, delta2;
+  const double *para;   // scheme parameters by slot
+  int p1, p2;           // boundary kind per axis (BC_PERIODIC / BC_WALL)
+  Status *status;       // device status block
+};
+
+enum StageKind : int {
+  STAGE_FIRST = 0,  // beta = 0: v is written, not read
+  STAGE_MID = 1,    // v read and written
+  STAGE_LAST = 2,   // v read, not written (dead until the next step's first stage)
+  STAGE_KICK = 3,   // the reference's kick(): v <- F(u) + beta v only, u untouched
+};
+
+// Tile geometry of the fused substage kernel for a storage type.
+struct TileShape {
+  int tw, th, threads;
+  size_t smem;
+};
+TileShape substage_tile(int storage);
+
+// Tensor map over one state array (all fields) in the device layout, with the box of
+// the substage kernel.  Returns CUDA_SUCCESS or the driver's error.
+CUresult encode_state_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
+
+cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_in_map, void *u_out, void *v,
+                            const Layout &L, const StageArgs &a, cudaStream_t s);
+
+cudaError_t launch_bcond(int storage, void *u, const Layout &L, int p1, int p2, cudaStream_t s);
+cudaError_t launch_drift(int storage, void *u, const void *v, const Layout &L, double dt, Status *status,
+                         cudaStream_t s);
+cudaError_t launch_euler(int storage, void *u, const Layout &L, double dt, const double *para, double delta1,
+                         double delta2, float r1, float r2, cudaStream_t s);
+cudaError_t launch_fill(int storage, void *p, size_t count, double value, cudaStream_t s);
+// host-layout rows [i0, i0 + nrows) (cell-interleaved, `host_double` selects double or
+// float elements) <-> the device layout
+cudaError_t launch_scatter(int storage, void *u, const void *src, bool host_double, const Layout &L, int i0,
+                           int nrows, cudaStream_t s);
+cudaError_t launch_gather(int storage, void *dst, const void *u, bool host_double, const Layout &L, int i0,
+                          int nrows, cudaStream_t s);
+// max over the interior of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2, in double, as
+// an atomic max into status->smax
+cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const double *para, double delta1,
+                              double delta2, Status *status, cudaStream_t s);
+// FP64 sums of the conserved densities, deterministic: partials[nblocks * 4] then out[4]
+int sums_blocks(const Layout &L);
+cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *partials, double *out,
+                        cudaStream_t s);
+// Device-resident time step: dt <- min(courant / smax, dt_diff, t_end - t), t <- t + dt
+// (applied by the caller's order: the update runs before the step that uses dt and
+// advances t by it), smax reset to 0 for the step's last stage to refill.
+cudaError_t launch_dt_update(Status *status, double courant, double dt_diff, double t_end, cudaStream_t s);
+
+}  // namespace fg2

@@ -1,0 +1,865 @@
+// fg2_b200/csrc/runtime.cpp -- host runtime and C ABI (include/fg2_b200.h), compiled once
+// per scheme with -I schemes/<name>.
+//
+// A simulation handle owns: two state arrays u[0], u[1] (ping-pong: a substage reads one
+// and writes the other, so no tile overwrites a halo a neighbouring tile still reads), the
+// RK3 register v, a tensor map per u array, a device status block and a stream.  The
+// reference keeps the same state in namespace global (src/global.cpp:22-31) and allocates
+// it in setup() (src/setup.cpp:60-87).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fg2_b200.h"
+#include "fg2b.h"
+#include "kernels.h"
+#include "setup_common.h"
+
+#include <state.h>
+#include <eqns.cuh>
+#include <Euler.cuh>
+#include <config.h>
+#include <init.h>
+
+using namespace fg2;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_status(cudaError_t e, const char *what)
+{
+  if (e == cudaSuccess) return FG2_OK;
+  return fail((int)e, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(expr)                                          \
+  do {                                                    \
+    cudaError_t e_ = (expr);                              \
+    if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
+  } while (0)
+
+size_t elem_size(int storage) { return storage == ST_F64 ? 8 : storage == ST_F32 ? 4 : 2; }
+size_t host_elem(int storage) { return storage == ST_F64 ? 8 : 4; }
+
+// RK3 coefficients (src/step.cpp:24-26), evaluated in double as the reference's E.
+const double RK_ALPHA[3] = {0.0, 1.0 / 3.0, 3.0 / 4.0};
+const double RK_BETA[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+const double RK_GAMMA[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+
+// 6th-order second-derivative symbol maximum (1088/180 per axis) and the RK3 real-axis
+// stability bound: the explicit diffusive limit is dt <= c_d * 2.51 / (D (6.04/D1^2 + 6.04/D2^2)).
+const double D2_SYMBOL = 1088.0 / 180.0;
+const double RK3_REAL_LIMIT = 2.51;
+
+}  // namespace
+
+struct fg2_sim {
+  int n1 = 0, n2 = 0, storage = ST_F32;
+  Layout L{};
+  void *u[2] = {nullptr, nullptr};
+  void *v = nullptr;
+  int cur = 0;  // u[cur] holds the state
+  CUtensorMap map[2];
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Status *status = nullptr;       // device
+  Status *status_host = nullptr;  // pinned mirror
+  double *sums_partial = nullptr, *sums_out = nullptr;
+  double para[8];
+  double l1 = 1.0, l2 = 1.0, c = 0.5;  // src/global.cpp:28
+  int p1 = 1, p2 = 1;                  // src/global.cpp:29
+  double delta1 = 0, delta2 = 0;
+  bool configured = false;
+  bool ghosts_valid = false;
+  bool smax_valid = false;
+  int dt_mode = FG2_DT_REFERENCE;
+  Rng forcing{0x5eed5eedull};
+  bool fixed_phases = false;
+  float r1 = 0.f, r2 = 0.f;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step graph per ping-pong parity
+  double graph_dt[2] = {0, 0}, graph_tend[2] = {0, 0};
+  char para_msg[256];
+  // the reference-mirror kick/drift may name arbitrary arrays: tensor map cache
+  const void *kick_map_base = nullptr;
+  CUtensorMap kick_map;
+};
+
+namespace {
+
+size_t array_elems(const fg2_sim *s) { return (size_t)scheme::NVAR * (size_t)s->L.PS; }
+
+// Delta = l / n in the state's precision (src/config.cpp:39: R Delta[] = {l1/n1, l2/n2}).
+void compute_deltas(fg2_sim *s)
+{
+  if (s->storage == ST_F64) {
+    s->delta1 = s->l1 / s->n1;
+    s->delta2 = s->l2 / s->n2;
+  } else {
+    s->delta1 = (double)((float)s->l1 / (float)s->n1);
+    s->delta2 = (double)((float)s->l2 / (float)s->n2);
+  }
+}
+
+// parameters are parsed into R like the reference's atof -> R (src/para.cpp:34)
+double round_para(const fg2_sim *s, double x) { return s->storage == ST_F64 ? x : (double)(float)x; }
+
+StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
+{
+  StageArgs a;
+  a.beta = RK_BETA[k];
+  a.gamma = RK_GAMMA[k];
+  a.dt = dt;
+  a.dt_dev = dt_dev;
+  a.delta1 = s->delta1;
+  a.delta2 = s->delta2;
+  a.para = s->para;
+  a.p1 = s->p1;
+  a.p2 = s->p2;
+  a.status = s->status;
+  return a;
+}
+
+bool supported_storage(int st) { return st == ST_F32 || st == ST_F64; }
+
+int ensure_config(fg2_sim *s)
+{
+  if (!s->configured) {
+    scheme::settings(s->l1, s->l2);
+    compute_deltas(s);
+    s->configured = true;
+  }
+  return FG2_OK;
+}
+
+int do_bcond(fg2_sim *s)
+{
+  CK(launch_bcond(s->storage, s->u[s->cur], s->L, s->p1, s->p2, s->stream));
+  s->ghosts_valid = true;
+  return FG2_OK;
+}
+
+int do_euler(fg2_sim *s, double dt)
+{
+  if (!s->fixed_phases) {  // the reference's RANDOMIZE: two phases per Euler call
+    s->r1 = (float)(6.2831853071795865 * s->forcing.uniform());
+    s->r2 = (float)(6.2831853071795865 * s->forcing.uniform());
+  }
+  CK(launch_euler(s->storage, s->u[s->cur], s->L, dt, s->para, s->delta1, s->delta2, s->r1, s->r2, s->stream));
+  s->ghosts_valid = false;
+  s->smax_valid = false;
+  return FG2_OK;
+}
+
+bool euler_active(const fg2_sim *s)
+{
+  Para<double> p;
+  for (int q = 0; q < 8; ++q) p.v[q] = s->para[q];
+  return scheme::euler_active<double>(p);
+}
+
+// One RK3 step: Euler hook, three fused substages.  dt_dev != null: device-resident dt.
+int enqueue_step(fg2_sim *s, double dt, const double *dt_dev, bool cfl)
+{
+  if (euler_active(s)) {
+    int rc = do_euler(s, dt);
+    if (rc) return rc;
+  }
+  if (!s->ghosts_valid) {
+    int rc = do_bcond(s);
+    if (rc) return rc;
+  }
+  for (int k = 0; k < 3; ++k) {
+    const StageArgs a = stage_args(s, k, dt, dt_dev);
+    const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
+    CK(launch_substage(s->storage, kind, cfl && k == 2, s->map[s->cur], s->u[1 - s->cur], s->v, s->L, a,
+                       s->stream));
+    s->cur = 1 - s->cur;
+  }
+  s->ghosts_valid = true;
+  s->smax_valid = cfl;
+  return FG2_OK;
+}
+
+double diffusive_dt(const fg2_sim *s)
+{
+  const double D = scheme::max_diffusivity(s->para);
+  if (D <= 0.0) return 0.0;
+  return s->c * RK3_REAL_LIMIT /
+         (D * D2_SYMBOL * (1.0 / (s->delta1 * s->delta1) + 1.0 / (s->delta2 * s->delta2)));
+}
+
+int read_status(fg2_sim *s)
+{
+  CK(cudaMemcpyAsync(s->status_host, s->status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  if (s->status_host->error) return fail(FG2_ERR_TIMEOUT, "a bounded in-kernel wait gave up (bits %u)", s->status_host->error);
+  if (s->status_host->nan) return fail(FG2_ERR_NAN, "NaN in the state");
+  return FG2_OK;
+}
+
+// host array (rows of n2 cells x NVAR values) <-> device layout, staged through the
+// spare ping-pong array (dead between steps) in row chunks.
+int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
+{
+  const size_t hrow = (size_t)s->n2 * scheme::NVAR * host_elem(s->storage);
+  const size_t cap = array_elems(s) * elem_size(s->storage);
+  const int rows_per = (int)std::min<size_t>((size_t)s->n1, cap / hrow);
+  if (rows_per < 1) return fail(FG2_ERR_ARG, "staging buffer too small");
+  void *stage = s->u[1 - s->cur];
+  if (dev_array == stage) return fail(FG2_ERR_ARG, "cannot stage through the target array");
+  const bool hd = s->storage == ST_F64;
+  for (int i0 = 0; i0 < s->n1; i0 += rows_per) {
+    const int nr = std::min(rows_per, s->n1 - i0);
+    char *h = (char *)host + (size_t)i0 * hrow;
+    if (to_device) {
+      CK(cudaMemcpyAsync(stage, h, nr * hrow, cudaMemcpyHostToDevice, s->stream));
+      CK(launch_scatter(s->storage, dev_array, stage, hd, s->L, i0, nr, s->stream));
+    } else {
+      CK(launch_gather(s->storage, stage, dev_array, hd, s->L, i0, nr, s->stream));
+      CK(cudaMemcpyAsync(h, stage, nr * hrow, cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+void drop_graph(fg2_sim *s)
+{
+  for (int b = 0; b < 2; ++b) {
+    if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
+    s->graph[b] = nullptr;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fg2_scheme_name(void) { return scheme::NAME; }
+int fg2_nvar(void) { return scheme::NVAR; }
+const char *fg2_field_name(int f) { return (f >= 0 && f < scheme::NVAR) ? scheme::FIELD_NAMES[f] : nullptr; }
+int fg2_eqns_flop(void) { return scheme::EQNS_FLOP; }
+int fg2_para_count(void) { return scheme::NSLOT; }
+const char *fg2_para_key(int k) { return (k >= 0 && k < scheme::NSLOT) ? scheme::PARA_KEYS[k].name : nullptr; }
+const char *fg2_last_error(void) { return g_err; }
+
+int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, const double *para, uint64_t seed,
+                       double *out)
+{
+  if (!name || !out || n1 < 1 || n2 < 1) return fail(FG2_ERR_ARG, "bad arguments");
+  double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < scheme::NSLOT; ++q)
+    p[scheme::PARA_KEYS[q].slot] = para ? para[q] : scheme::PARA_KEYS[q].def;
+  scheme::settings(l1, l2);
+  SetupCtx ctx{n1, n2, l1, l2, p, seed};
+  std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
+  const size_t row = (size_t)n2 * scheme::NVAR;
+  for (int i = 0; i < n1; ++i) {
+    if (setup) setup->row(i, out + (size_t)i * row);
+    else std::memset(out + (size_t)i * row, 0, row * sizeof(double));
+  }
+  return setup ? 1 : 0;
+}
+
+fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
+{
+  if (n1 < HALF || n2 < HALF) {
+    fail(FG2_ERR_ARG, "grid %d x %d is smaller than the ghost width %d", n1, n2, HALF);
+    return nullptr;
+  }
+  if (!supported_storage(storage)) {
+    fail(FG2_ERR_UNSUPPORTED, "storage %d is not supported by the plain path", storage);
+    return nullptr;
+  }
+  std::unique_ptr<fg2_sim> s(new fg2_sim);
+  s->n1 = n1;
+  s->n2 = n2;
+  s->storage = storage;
+  s->L = make_layout(n1, n2, elem_size(storage));
+  for (int q = 0; q < 8; ++q) s->para[q] = 0.0;
+  for (int q = 0; q < scheme::NSLOT; ++q) s->para[scheme::PARA_KEYS[q].slot] = round_para(s.get(), scheme::PARA_KEYS[q].def);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      fail(FG2_ERR_ALLOC, "stream creation failed");
+      return nullptr;
+    }
+    s->own_stream = true;
+  }
+  const size_t bytes = array_elems(s.get()) * elem_size(storage);
+  auto cleanup = [&](const char *what) {
+    fail(FG2_ERR_ALLOC, "%s", what);
+    fg2_sim_destroy(s.release());
+    return nullptr;
+  };
+  if (cudaMalloc(&s->u[0], bytes) != cudaSuccess || cudaMalloc(&s->u[1], bytes) != cudaSuccess ||
+      cudaMalloc(&s->v, bytes) != cudaSuccess)
+    return cleanup("device allocation of the state failed");
+  if (cudaMalloc(&s->status, sizeof(Status)) != cudaSuccess ||
+      cudaMallocHost(&s->status_host, sizeof(Status)) != cudaSuccess)
+    return cleanup("status allocation failed");
+  if (cudaMalloc(&s->sums_partial, sizeof(double) * 4 * sums_blocks(s->L)) != cudaSuccess ||
+      cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess)
+    return cleanup("reduction scratch allocation failed");
+  for (int b = 0; b < 2; ++b)
+    if (encode_state_map(&s->map[b], s->u[b], s->L, storage) != CUDA_SUCCESS) {
+      fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
+      fg2_sim_destroy(s.release());
+      return nullptr;
+    }
+  // every array starts at -max like the reference (src/setup.cpp:80-83)
+  const double lowest = storage == ST_F64 ? -std::numeric_limits<double>::max() : -std::numeric_limits<float>::max();
+  if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
+      launch_fill(storage, s->u[1], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
+      launch_fill(storage, s->v, array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->status, 0, sizeof(Status), s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return cleanup("initial fill failed");
+  return s.release();
+}
+
+void fg2_sim_destroy(fg2_sim *s)
+{
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graph(s);
+  cudaFree(s->u[0]);
+  cudaFree(s->u[1]);
+  cudaFree(s->v);
+  cudaFree(s->status);
+  cudaFreeHost(s->status_host);
+  cudaFree(s->sums_partial);
+  cudaFree(s->sums_out);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+size_t fg2_sim_device_bytes(const fg2_sim *s) { return s ? 3 * array_elems(s) * elem_size(s->storage) : 0; }
+int fg2_sim_storage(const fg2_sim *s) { return s ? s->storage : -1; }
+
+int fg2_sim_set_box(fg2_sim *s, double l1, double l2)
+{
+  if (!s || !(l1 > 0) || !(l2 > 0)) return fail(FG2_ERR_ARG, "box sizes must be positive");
+  s->l1 = round_para(s, l1);
+  s->l2 = round_para(s, l2);
+  s->configured = false;
+  drop_graph(s);
+  return FG2_OK;
+}
+
+int fg2_sim_set_courant(fg2_sim *s, double c)
+{
+  if (!s || !(c > 0)) return fail(FG2_ERR_ARG, "Courant number must be positive");
+  s->c = round_para(s, c);
+  drop_graph(s);
+  return FG2_OK;
+}
+
+int fg2_sim_set_bcond(fg2_sim *s, int p1, int p2)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  s->p1 = p1 ? BC_PERIODIC : BC_WALL;
+  s->p2 = p2 ? BC_PERIODIC : BC_WALL;
+  s->ghosts_valid = false;
+  drop_graph(s);
+  return FG2_OK;
+}
+
+const char *fg2_sim_para(fg2_sim *s, const char *in)
+{
+  if (!s || !in) return nullptr;
+  while (*in == '-') ++in;  // skip leading dashes (src/para.cpp:30)
+  const char *eq = std::strchr(in, '=');
+  if (!eq) { fail(FG2_ERR_ARG, "expected key=val"); return nullptr; }
+  const std::string key(in, eq - in);
+  for (int q = 0; q < scheme::NSLOT; ++q)
+    if (key == scheme::PARA_KEYS[q].name) {
+      const double val = round_para(s, std::atof(eq + 1));
+      s->para[scheme::PARA_KEYS[q].slot] = val;
+      snprintf(s->para_msg, sizeof(s->para_msg), "%s = %g", key.c_str(), val);
+      drop_graph(s);
+      return s->para_msg;
+    }
+  fail(FG2_ERR_ARG, "unknown parameter '%s' for scheme %s", key.c_str(), scheme::NAME);
+  return nullptr;
+}
+
+int fg2_sim_get_para(const fg2_sim *s, const char *key, double *val)
+{
+  if (!s || !key || !val) return fail(FG2_ERR_ARG, "null argument");
+  for (int q = 0; q < scheme::NSLOT; ++q)
+    if (!std::strcmp(key, scheme::PARA_KEYS[q].name)) {
+      *val = s->para[scheme::PARA_KEYS[q].slot];
+      return FG2_OK;
+    }
+  return fail(FG2_ERR_ARG, "unknown parameter '%s'", key);
+}
+
+int fg2_sim_config(fg2_sim *s)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  s->configured = false;
+  drop_graph(s);
+  return ensure_config(s);
+}
+
+int fg2_sim_init(fg2_sim *s, const char *name, uint64_t seed)
+{
+  if (!s || !name) return fail(FG2_ERR_ARG, "null argument");
+  ensure_config(s);
+  SetupCtx ctx{s->n1, s->n2, s->l1, s->l2, s->para, seed};
+  std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
+  const size_t ncell = (size_t)s->n2 * scheme::NVAR;
+  std::vector<double> row(ncell, 0.0);
+  const bool hd = s->storage == ST_F64;
+  std::vector<unsigned char> host((size_t)s->n1 * ncell * host_elem(s->storage));
+  for (int i = 0; i < s->n1; ++i) {
+    if (setup) setup->row(i, row.data());
+    if (hd) std::memcpy(host.data() + (size_t)i * ncell * 8, row.data(), ncell * 8);
+    else {
+      float *h = (float *)host.data() + (size_t)i * ncell;
+      for (size_t k = 0; k < ncell; ++k) h[k] = (float)row[k];
+    }
+  }
+  return fg2_sim_upload(s, host.data());
+}
+
+int fg2_sim_upload(fg2_sim *s, const void *host)
+{
+  if (!s || !host) return fail(FG2_ERR_ARG, "null argument");
+  int rc = transfer(s, s->u[s->cur], const_cast<void *>(host), true);
+  s->ghosts_valid = false;
+  s->smax_valid = false;
+  return rc;
+}
+
+int fg2_sim_download(fg2_sim *s, void *host)
+{
+  if (!s || !host) return fail(FG2_ERR_ARG, "null argument");
+  return transfer(s, s->u[s->cur], host, false);
+}
+
+int fg2_sim_upload_v(fg2_sim *s, const void *host)
+{
+  if (!s || !host) return fail(FG2_ERR_ARG, "null argument");
+  return transfer(s, s->v, const_cast<void *>(host), true);
+}
+
+int fg2_sim_download_v(fg2_sim *s, void *host)
+{
+  if (!s || !host) return fail(FG2_ERR_ARG, "null argument");
+  return transfer(s, s->v, host, false);
+}
+
+int fg2_sim_set_dt_mode(fg2_sim *s, int mode)
+{
+  if (!s || (mode != FG2_DT_REFERENCE && mode != FG2_DT_CFL)) return fail(FG2_ERR_ARG, "bad dt mode");
+  s->dt_mode = mode;
+  return FG2_OK;
+}
+
+double fg2_sim_getdt(fg2_sim *s)
+{
+  if (!s) return 0.0;
+  ensure_config(s);
+  if (s->dt_mode == FG2_DT_REFERENCE) {
+    // (E)c / (n1 / l1 + n2 / l2) with the quotients in R (src/getdt.cpp:26)
+    if (s->storage == ST_F64) return s->c / (s->n1 / s->l1 + s->n2 / s->l2);
+    const float den = (float)s->n1 / (float)s->l1 + (float)s->n2 / (float)s->l2;
+    return (double)(float)s->c / (double)den;
+  }
+  if (cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream) != cudaSuccess ||
+      launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(s->status_host, s->status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    fail(FG2_ERR_ARG, "getdt reduction failed");
+    return 0.0;
+  }
+  s->smax_valid = true;
+  unsigned long long bits = s->status_host->smax;
+  double smax;
+  std::memcpy(&smax, &bits, sizeof(smax));
+  double dt = smax > 0 ? s->c / smax : std::numeric_limits<double>::infinity();
+  const double dd = diffusive_dt(s);
+  if (dd > 0 && dd < dt) dt = dd;
+  return dt;
+}
+
+int fg2_sim_step(fg2_sim *s, double t, double dt)
+{
+  (void)t;  // passed to the equations by the reference but unused by them (src/kick.cu:98)
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  ensure_config(s);
+  int rc = enqueue_step(s, dt, nullptr, false);
+  if (rc) return rc;
+  return read_status(s);
+}
+
+int fg2_sim_advance(fg2_sim *s, int nsteps, double dt, double t_end)
+{
+  if (!s || nsteps < 0) return fail(FG2_ERR_ARG, "bad arguments");
+  ensure_config(s);
+  const bool device_dt = !(dt > 0);
+  if (device_dt && !s->smax_valid) {
+    CK(cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream));
+    CK(launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream));
+    s->smax_valid = true;
+  }
+  for (int n = 0; n < nsteps; ++n) {
+    if (device_dt) CK(launch_dt_update(s->status, s->c, diffusive_dt(s), t_end, s->stream));
+    int rc = enqueue_step(s, dt, device_dt ? &s->status->dt : nullptr, device_dt);
+    if (rc) return rc;
+  }
+  return FG2_OK;
+}
+
+int fg2_sim_advance_graph(fg2_sim *s, int nsteps, double dt, double t_end)
+{
+  if (!s || nsteps < 0) return fail(FG2_ERR_ARG, "bad arguments");
+  if (euler_active(s) && !s->fixed_phases)
+    return fail(FG2_ERR_UNSUPPORTED, "per-step random forcing phases cannot be replayed from a graph");
+  ensure_config(s);
+  const bool device_dt = !(dt > 0);
+  // bring the state to a point every replay starts from: valid ghosts and signal max
+  if (!s->ghosts_valid || euler_active(s)) {
+    int rc = fg2_sim_advance(s, 1, dt, t_end);
+    if (rc) return rc;
+    --nsteps;
+  }
+  if (device_dt && !s->smax_valid) {
+    int rc = fg2_sim_advance(s, 1, dt, t_end);
+    if (rc) return rc;
+    --nsteps;
+  }
+  if (nsteps <= 0) return FG2_OK;
+  const int b = s->cur;
+  if (s->graph[b] && (s->graph_dt[b] != dt || s->graph_tend[b] != t_end)) {
+    cudaGraphExecDestroy(s->graph[b]);
+    s->graph[b] = nullptr;
+  }
+  if (!s->graph[b]) {
+    // two steps = six substages: the ping-pong parity returns to the start
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = fg2_sim_advance(s, 2, dt, t_end);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc) return rc;
+    CK(e);
+    e = cudaGraphInstantiate(&s->graph[b], g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    s->graph_dt[b] = dt;
+    s->graph_tend[b] = t_end;
+  }
+  for (int n = 0; n + 1 < nsteps; n += 2) CK(cudaGraphLaunch(s->graph[b], s->stream));
+  if (nsteps & 1) return fg2_sim_advance(s, 1, dt, t_end);
+  return FG2_OK;
+}
+
+int fg2_sim_stage(fg2_sim *s, int k, double dt)
+{
+  if (!s || k < 0 || k > 2) return fail(FG2_ERR_ARG, "bad arguments");
+  ensure_config(s);
+  if (!s->ghosts_valid) {
+    int rc = do_bcond(s);
+    if (rc) return rc;
+  }
+  const StageArgs a = stage_args(s, k, dt, nullptr);
+  const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
+  CK(launch_substage(s->storage, kind, false, s->map[s->cur], s->u[1 - s->cur], s->v, s->L, a, s->stream));
+  s->cur = 1 - s->cur;
+  s->smax_valid = false;
+  return FG2_OK;
+}
+
+int fg2_sim_sync(fg2_sim *s)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  return read_status(s);
+}
+
+int fg2_sim_set_time(fg2_sim *s, double t)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  CK(cudaMemcpyAsync(&s->status->t, &t, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+double fg2_sim_time(fg2_sim *s)
+{
+  if (!s || read_status(s) < 0) return NAN;
+  return s->status_host->t;
+}
+
+double fg2_sim_last_dt(fg2_sim *s)
+{
+  if (!s || read_status(s) < 0) return NAN;
+  return s->status_host->dt_next;
+}
+
+void fg2_sim_clear_status(fg2_sim *s)
+{
+  if (!s) return;
+  cudaMemsetAsync(s->status, 0, 2 * sizeof(unsigned), s->stream);
+  cudaStreamSynchronize(s->stream);
+}
+
+int fg2_sim_kick(fg2_sim *s, double t, double beta)
+{
+  (void)t;
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  ensure_config(s);
+  StageArgs a = stage_args(s, 0, 0.0, nullptr);
+  a.beta = beta;
+  CK(launch_substage(s->storage, STAGE_KICK, false, s->map[s->cur], nullptr, s->v, s->L, a, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+int fg2_sim_drift(fg2_sim *s, double dt)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  const double r = s->storage == ST_F64 ? dt : (double)(float)dt;
+  CK(launch_drift(s->storage, s->u[s->cur], s->v, s->L, r, s->status, s->stream));
+  s->ghosts_valid = false;
+  s->smax_valid = false;
+  return read_status(s);
+}
+
+int fg2_sim_bcond(fg2_sim *s)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  int rc = do_bcond(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+int fg2_sim_euler(fg2_sim *s, double dt)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  ensure_config(s);
+  int rc = do_euler(s, dt);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+int fg2_sim_set_forcing_phases(fg2_sim *s, double r1, double r2)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  s->fixed_phases = true;
+  s->r1 = (float)r1;
+  s->r2 = (float)r2;
+  drop_graph(s);
+  return FG2_OK;
+}
+
+int fg2_sim_seed_forcing(fg2_sim *s, uint64_t seed)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  s->fixed_phases = false;
+  s->forcing = Rng(seed);
+  drop_graph(s);
+  return FG2_OK;
+}
+
+int fg2_sim_sums(fg2_sim *s, double out[4])
+{
+  if (!s || !out) return fail(FG2_ERR_ARG, "null argument");
+  CK(launch_sums(s->storage, s->u[s->cur], s->L, s->sums_partial, s->sums_out, s->stream));
+  CK(cudaMemcpyAsync(out, s->sums_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
+void *fg2_sim_u(fg2_sim *s) { return s ? s->u[s->cur] : nullptr; }
+void *fg2_sim_v(fg2_sim *s) { return s ? s->v : nullptr; }
+void *fg2_sim_stream(fg2_sim *s) { return s ? (void *)s->stream : nullptr; }
+
+int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  if (pitch) *pitch = s->L.P;
+  if (plane) *plane = s->L.PS;
+  return FG2_OK;
+}
+
+// .raw frames (src/io.cpp:24-76): int[6] {n1, n2, NVAR, sizeof(R), p1, p2}, E time,
+// R[3] {l1, l2, c}, then n1 * n2 * NVAR values of R without ghosts.  E is double for
+// R = float and long double for R = double (src/fg2.h:36-45).
+int fg2_sim_dump(fg2_sim *s, const char *path, double time)
+{
+  if (!s || !path) return fail(FG2_ERR_ARG, "null argument");
+  const bool hd = s->storage == ST_F64;
+  const size_t he = host_elem(s->storage);
+  std::vector<unsigned char> data((size_t)s->n1 * s->n2 * scheme::NVAR * he);
+  int rc = fg2_sim_download(s, data.data());
+  if (rc) return rc;
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(FG2_ERR_ARG, "cannot open %s", path);
+  const int size[6] = {s->n1, s->n2, scheme::NVAR, (int)he, s->p1, s->p2};
+  bool ok = std::fwrite(size, sizeof(int), 6, f) == 6;
+  if (hd) {
+    const long double t = time;
+    const double info[3] = {s->l1, s->l2, s->c};
+    ok = ok && std::fwrite(&t, sizeof(t), 1, f) == 1 && std::fwrite(info, sizeof(double), 3, f) == 3;
+  } else {
+    const float info[3] = {(float)s->l1, (float)s->l2, (float)s->c};
+    ok = ok && std::fwrite(&time, sizeof(double), 1, f) == 1 && std::fwrite(info, sizeof(float), 3, f) == 3;
+  }
+  ok = ok && std::fwrite(data.data(), 1, data.size(), f) == data.size();
+  std::fclose(f);
+  return ok ? FG2_OK : fail(FG2_ERR_ARG, "short write to %s", path);
+}
+
+int fg2_sim_load(fg2_sim *s, const char *path, double *time)
+{
+  if (!s || !path) return fail(FG2_ERR_ARG, "null argument");
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(FG2_ERR_ARG, "cannot open %s", path);
+  const bool hd = s->storage == ST_F64;
+  const size_t he = host_elem(s->storage);
+  int size[6];
+  bool ok = std::fread(size, sizeof(int), 6, f) == 6;
+  // compatibility check of src/io.cpp:32-33
+  if (!ok || size[0] != s->n1 || size[1] != s->n2 || size[2] != scheme::NVAR || size[3] != (int)he) {
+    std::fclose(f);
+    return fail(FG2_ERR_ARG, "input data is not compatible with the setup");
+  }
+  double t = 0;
+  if (hd) {
+    long double lt;
+    double info[3];
+    ok = std::fread(&lt, sizeof(lt), 1, f) == 1 && std::fread(info, sizeof(double), 3, f) == 3;
+    t = (double)lt;
+    s->l1 = info[0]; s->l2 = info[1]; s->c = info[2];
+  } else {
+    float info[3];
+    ok = std::fread(&t, sizeof(double), 1, f) == 1 && std::fread(info, sizeof(float), 3, f) == 3;
+    s->l1 = info[0]; s->l2 = info[1]; s->c = info[2];
+  }
+  std::vector<unsigned char> data((size_t)s->n1 * s->n2 * scheme::NVAR * he);
+  ok = ok && std::fread(data.data(), 1, data.size(), f) == data.size();
+  std::fclose(f);
+  if (!ok) return fail(FG2_ERR_ARG, "short read from %s", path);
+  s->p1 = size[4] ? BC_PERIODIC : BC_WALL;
+  s->p2 = size[5] ? BC_PERIODIC : BC_WALL;
+  s->configured = false;
+  drop_graph(s);
+  if (time) *time = t;
+  return fg2_sim_upload(s, data.data());
+}
+
+// ---- reference-mirror API over one process-wide simulation ------------------------------
+static fg2_sim *g_sim = nullptr;
+static void g_done(void) { fg2_sim_destroy(g_sim); g_sim = nullptr; }
+
+fg2_sim *fg2_global(void) { return g_sim; }
+
+size_t fg2_setup(int n1, int n2)
+{
+  if (g_sim) g_done();
+  else std::atexit(g_done);  // the reference frees in an atexit hook (src/setup.cpp:24-34)
+  g_sim = fg2_sim_create(n1, n2, ST_F32, nullptr);
+  return g_sim ? fg2_sim_device_bytes(g_sim) : 0;
+}
+
+void fg2_config(void) { if (g_sim) fg2_sim_config(g_sim); }
+const char *fg2_para(const char *in) { return g_sim ? fg2_sim_para(g_sim, in) : nullptr; }
+void fg2_init(const char *name) { if (g_sim) fg2_sim_init(g_sim, name, 0); }
+
+double fg2_load(const char *path)
+{
+  double t = 0;
+  if (g_sim) fg2_sim_load(g_sim, path, &t);
+  return t;
+}
+
+void fg2_dump(const char *path, double time) { if (g_sim) fg2_sim_dump(g_sim, path, time); }
+double fg2_getdt(void) { return g_sim ? fg2_sim_getdt(g_sim) : 0.0; }
+int fg2_step(double t, double dt) { return g_sim ? fg2_sim_step(g_sim, t, dt) : FG2_ERR_ARG; }
+
+// kick/drift/bcond/Euler take device pointers into arrays of the global layout, as the
+// reference's take interior-origin pointers (src/fg2.h:81-84).
+static int array_index(const void *p)
+{
+  if (!g_sim) return -1;
+  if (p == g_sim->u[0]) return 0;
+  if (p == g_sim->u[1]) return 1;
+  if (p == g_sim->v) return 2;
+  return -1;
+}
+
+void fg2_kick(float *v, const float *u, float t, float beta)
+{
+  (void)t;
+  if (!g_sim) return;
+  ensure_config(g_sim);
+  const int ui = array_index(u);
+  const CUtensorMap *m = nullptr;
+  if (ui == 0 || ui == 1) m = &g_sim->map[ui];
+  else {
+    if (g_sim->kick_map_base != u) {
+      if (encode_state_map(&g_sim->kick_map, u, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
+      g_sim->kick_map_base = u;
+    }
+    m = &g_sim->kick_map;
+  }
+  StageArgs a = stage_args(g_sim, 0, 0.0, nullptr);
+  a.beta = beta;
+  launch_substage(g_sim->storage, STAGE_KICK, false, *m, nullptr, v, g_sim->L, a, g_sim->stream);
+  cudaStreamSynchronize(g_sim->stream);
+}
+
+void fg2_drift(float *u, const float *v, float dt)
+{
+  if (!g_sim) return;
+  launch_drift(g_sim->storage, u, v, g_sim->L, dt, g_sim->status, g_sim->stream);
+  if (u == g_sim->u[g_sim->cur]) { g_sim->ghosts_valid = false; g_sim->smax_valid = false; }
+  cudaStreamSynchronize(g_sim->stream);
+}
+
+void fg2_bcond(float *u, int p1, int p2)
+{
+  if (!g_sim) return;
+  launch_bcond(g_sim->storage, u, g_sim->L, p1 ? BC_PERIODIC : BC_WALL, p2 ? BC_PERIODIC : BC_WALL, g_sim->stream);
+  cudaStreamSynchronize(g_sim->stream);
+}
+
+void fg2_Euler(float *u, float dt)
+{
+  if (!g_sim) return;
+  ensure_config(g_sim);
+  if (!g_sim->fixed_phases) {
+    g_sim->r1 = (float)(6.2831853071795865 * g_sim->forcing.uniform());
+    g_sim->r2 = (float)(6.2831853071795865 * g_sim->forcing.uniform());
+  }
+  launch_euler(g_sim->storage, u, g_sim->L, dt, g_sim->para, g_sim->delta1, g_sim->delta2, g_sim->r1, g_sim->r2,
+               g_sim->stream);
+  cudaStreamSynchronize(g_sim->stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+/*
+ * include/fg2_b200.h -- C ABI of the B200-native fg2 time step.
+ *
+ * One shared library per scheme, as the reference builds one binary per scheme directory
+ * (Makefile:19-22, `make hydro` -> bin/hydro): libfg2_hydro.so and libfg2_hydro-isot.so
+ * export the same symbols.  Plain C types only; device pointers are `void *`.
+ *
+ * Two layers:
+ *   - the handle API (fg2_sim_*): explicit simulation objects, a caller-chosen CUDA stream,
+ *     status codes instead of exit();
+ *   - the reference-mirror API (fg2_setup ... fg2_Euler): the function contract of
+ *     src/fg2.h:60-84 over one process-wide simulation, with the reference's argument
+ *     meanings and return conventions.
+ *
+ * Status codes: 0 success; 1 a NaN appeared (the reference returns cudaErrorInvalidValue,
+ * whose value is 1, src/step.cpp:38-40); other positive values are cudaError_t codes;
+ * negative values are the FG2_ERR_* library errors below.
+ *
+ * Host arrays exchanged with the library use the reference's host layout without ghosts
+ * (src/init.cpp:39-41, src/io.cpp:41-44): n1 * n2 cells in row-major order (axis 2
+ * contiguous), NVAR interleaved values per cell, of type float (storage FG2_F32, FG2_F16,
+ * FG2_BF16) or double (FG2_F64).
+ */
+#ifndef FG2_B200_H
+#define FG2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FG2_OK 0
+#define FG2_ERR_NAN 1         /* == cudaErrorInvalidValue, the reference's NaN status */
+#define FG2_ERR_ARG (-1)      /* bad argument (size, key, mode) */
+#define FG2_ERR_ALLOC (-2)    /* device or host allocation failed */
+#define FG2_ERR_TMA (-3)      /* tensor-map encoding failed */
+#define FG2_ERR_TIMEOUT (-4)  /* a bounded in-kernel wait gave up */
+#define FG2_ERR_UNSUPPORTED (-5)
+
+/* State storage precision. */
+#define FG2_F32 0
+#define FG2_F64 1
+#define FG2_F16 2
+#define FG2_BF16 3
+
+/* getdt() modes. */
+#define FG2_DT_REFERENCE 0 /* c / (n1/l1 + n2/l2), src/getdt.cpp:26 */
+#define FG2_DT_CFL 1       /* FP64 reduction: c / max[(|u1|+cs)/D1 + (|u2|+cs)/D2], capped by the diffusive limit */
+
+typedef struct fg2_sim fg2_sim;
+
+/* ---- scheme description (compile-time plug-in, src/fg2.h:47-48, <scheme>/config.h) ---- */
+const char *fg2_scheme_name(void);
+int fg2_nvar(void);                 /* NVAR = sizeof(S) / sizeof(R), src/fg2.h:48 */
+const char *fg2_field_name(int f);  /* field order of <scheme>/state.h */
+int fg2_eqns_flop(void);            /* eqns_flop, src/hydro/config.h:19 */
+int fg2_para_count(void);
+const char *fg2_para_key(int k);    /* the para_<key> names of <scheme>/eqns.cuh */
+const char *fg2_last_error(void);   /* text of the last library error (thread-local) */
+/* Evaluate a named initial condition on the host (no device needed): fills out[n1*n2*NVAR]
+ * in the host layout, in double.  para: the scheme's parameter values in the order of
+ * fg2_para_key(), or NULL for the defaults.  Returns 1 for a known name, 0 for an
+ * unknown one (zeros, like the reference's pick() default), negative on bad arguments. */
+int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, const double *para, uint64_t seed,
+                       double *out);
+
+/* ---- handle API ------------------------------------------------------------------------ */
+/* setup() (src/setup.cpp:32-87): allocates u (two ping-pong arrays) and v on the current
+ * device.  stream: a cudaStream_t, or NULL for a stream the handle owns.  NULL on failure. */
+fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream);
+void fg2_sim_destroy(fg2_sim *s);
+size_t fg2_sim_device_bytes(const fg2_sim *s);
+int fg2_sim_storage(const fg2_sim *s);
+/* global::l1/l2, c, p1/p2 (src/global.cpp:22-31; set by -l, -c, -b in src/main.cpp:48-57) */
+int fg2_sim_set_box(fg2_sim *s, double l1, double l2);
+int fg2_sim_set_courant(fg2_sim *s, double c);
+int fg2_sim_set_bcond(fg2_sim *s, int p1, int p2);
+/* para() (src/para.cpp:25-40): "key=val" (leading dashes skipped); returns "key = val" in a
+ * buffer owned by the handle, or NULL for an unknown key. */
+const char *fg2_sim_para(fg2_sim *s, const char *keyval);
+int fg2_sim_get_para(const fg2_sim *s, const char *key, double *val);
+/* config() (src/config.cpp:24-42): scheme settings() then Delta1/Delta2 = l / n. */
+int fg2_sim_config(fg2_sim *s);
+/* init() (src/init.cpp:26-42): evaluate the named setup at cell centres on the host and
+ * copy it to the device.  Unknown names give zeros, as the reference's pick() does.
+ * `seed` seeds every random draw of the setup.  Names may carry options:
+ * "turb:mach=0.3,kmin=2,kmax=16", "noise:sigma=0.01", "kh:w=0.01". */
+int fg2_sim_init(fg2_sim *s, const char *name, uint64_t seed);
+int fg2_sim_upload(fg2_sim *s, const void *host);   /* host array -> u */
+int fg2_sim_download(fg2_sim *s, void *host);       /* u -> host array */
+int fg2_sim_upload_v(fg2_sim *s, const void *host); /* host array -> v */
+int fg2_sim_download_v(fg2_sim *s, void *host);     /* v -> host array */
+/* getdt() (src/getdt.cpp:22-29) in the selected mode; FG2_DT_CFL synchronises. */
+int fg2_sim_set_dt_mode(fg2_sim *s, int mode);
+double fg2_sim_getdt(fg2_sim *s);
+/* step() (src/step.cpp:22-43): Euler hook, then three fused RK3 substages; synchronises
+ * and returns the status (1 on NaN). */
+int fg2_sim_step(fg2_sim *s, double t, double dt);
+/* nsteps steps enqueued on the stream without synchronising.  dt > 0: fixed dt.
+ * dt <= 0: device-resident CFL time step (getdt fused into the last substage), advancing
+ * the device clock toward t_end (steps past t_end do nothing). */
+int fg2_sim_advance(fg2_sim *s, int nsteps, double dt, double t_end);
+/* The same through a CUDA graph of two steps, captured on first use and replayed. */
+int fg2_sim_advance_graph(fg2_sim *s, int nsteps, double dt, double t_end);
+/* One fused RK3 substage k (0, 1, 2) of a step with time step dt, enqueued without
+ * synchronising (src/step.cpp:30-35: bcond, kick, drift of stage k in one pass). */
+int fg2_sim_stage(fg2_sim *s, int k, double dt);
+int fg2_sim_sync(fg2_sim *s);                 /* wait; status of everything enqueued */
+int fg2_sim_set_time(fg2_sim *s, double t);   /* device clock for device-resident runs */
+double fg2_sim_time(fg2_sim *s);              /* device clock (synchronises) */
+double fg2_sim_last_dt(fg2_sim *s);           /* last device-chosen dt (synchronises) */
+void fg2_sim_clear_status(fg2_sim *s);        /* clear the sticky NaN / error words */
+/* The reference's building blocks on the handle's current arrays. */
+int fg2_sim_kick(fg2_sim *s, double t, double beta); /* v <- F(u) + beta v  (src/kick.cu:108-114) */
+int fg2_sim_drift(fg2_sim *s, double dt);            /* u <- u + dt v        (src/drift.cu:34-39) */
+int fg2_sim_bcond(fg2_sim *s);                       /* ghost fill           (src/bcond.cu:77-86) */
+int fg2_sim_euler(fg2_sim *s, double dt);            /* Euler hook           (src/kick.cu:128-138) */
+/* Random phases of the stochastic forcing (src/hydro-isot/Euler.cuh:39-44).  After this
+ * call every step uses (r1, r2); fg2_sim_seed_forcing returns to seeded per-step draws. */
+int fg2_sim_set_forcing_phases(fg2_sim *s, double r1, double r2);
+int fg2_sim_seed_forcing(fg2_sim *s, uint64_t seed);
+/* FP64 sums of rho, rho u1, rho u2 and the energy density over the interior, in a fixed
+ * reduction order (bitwise reproducible). */
+int fg2_sim_sums(fg2_sim *s, double out[4]);
+/* Current device arrays and their layout: element (f, i, j) at
+ * base[f * plane + (i + 3) * pitch + (j + 4)], elements of the storage type. */
+void *fg2_sim_u(fg2_sim *s);
+void *fg2_sim_v(fg2_sim *s);
+int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane);
+void *fg2_sim_stream(fg2_sim *s);
+/* dump()/load() (src/io.cpp:24-76): the reference's .raw frame format. */
+int fg2_sim_dump(fg2_sim *s, const char *path, double time);
+int fg2_sim_load(fg2_sim *s, const char *path, double *time);
+
+/* ---- reference-mirror API (src/fg2.h:60-84) over one process-wide simulation ------------ */
+size_t fg2_setup(int n1, int n2);          /* bytes of device memory, 0 on failure */
+void fg2_config(void);
+const char *fg2_para(const char *keyval);
+void fg2_init(const char *name);
+double fg2_load(const char *path);
+void fg2_dump(const char *path, double time);
+double fg2_getdt(void);
+int fg2_step(double t, double dt);
+void fg2_kick(float *v, const float *u, float t, float beta);
+void fg2_drift(float *u, const float *v, float dt);
+void fg2_bcond(float *u, int p1, int p2);
+void fg2_Euler(float *u, float dt);
+fg2_sim *fg2_global(void);                 /* the process-wide simulation (global::u, v, ...) */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FG2_B200_H */

@@ -1,0 +1,151 @@
+/*
+ * oracle/ref_harness.cpp -- TEST INFRASTRUCTURE ONLY (never linked into the product).
+ *
+ * Compiles the reference's OWN per-cell arithmetic for the host: src/fg2.h (types),
+ * src/deriv.h (the 6th-order stencil macros), <scheme>/state.h, <scheme>/eqns.cuh
+ * (right-hand side), <scheme>/Euler.cuh and <scheme>/bcond.cuh, included in place from
+ * the reference tree by oracle/Makefile (-I$(REF)/src -I$(REF)/src/<scheme>).  Nothing
+ * of the reference is copied here: this file only provides the host stand-ins for the
+ * CUDA qualifiers and the loops (oracle/loops.h), and exports the same C API as
+ * oracle/port.cpp so that the two can be compared call for call.
+ *
+ * The output goes to oracle/_ref/ and is used to pin the port (golden vectors in
+ * tests/golden/) and as the reference CPU baseline of bench.py.
+ */
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <cstdio>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// Host stand-ins for the CUDA qualifiers used by the included headers.
+#define __device__
+#define __constant__
+#define __global__
+// The reference calls unqualified exp/cos/sin/sqrt on R; on the device R=float picks
+// the float functions, so the host build must see the float overloads too.
+using std::cos;
+using std::exp;
+using std::sin;
+using std::sqrt;
+
+// src/hydro/bcond.cuh and src/hydro-isot/bcond.cuh select the variable by threadIdx.x.
+static struct { int x, y, z; } threadIdx;
+
+#include "fg2.h"   // src/fg2.h: R, E, K(), S, NVAR, HALF; pulls <state.h>
+#include "deriv.h" // src/deriv.h: Delta1, Delta2, D1 D2 D11 D22 D12
+#include <eqns.cuh>
+#include <Euler.cuh>
+#include <bcond.cuh>
+
+#define NV ((int)NVAR)
+
+#define orc_eqns(c, i, j, s) eqns((c), (i), (j), (s))
+#define orc_first_order(c, dt, i, j) first_order((c), (dt), (i), (j))
+static inline R ref_transform(int var, R x)
+{
+  threadIdx.x = var;
+  return transform(x);
+}
+#define orc_transform(var, x) ref_transform((var), (x))
+#include "loops.h"
+
+namespace {
+struct Key { const char *name; R *val; };
+#if defined(FG2_SCHEME_HYDRO)
+Key keys[] = {{"gamma", &para_gamma}, {"nus", &para_nus}, {"nub", &para_nub},
+              {"kappa", &para_kappa}, {"dd", &para_dd}};
+#elif defined(FG2_SCHEME_ISOT)
+Key keys[] = {{"dd", &para_dd}, {"nus", &para_nus}, {"nub", &para_nub},
+              {"cs2", &para_cs2}, {"f", &para_f}, {"k", &para_k}};
+#else
+#error "define FG2_SCHEME_HYDRO or FG2_SCHEME_ISOT"
+#endif
+}  // namespace
+
+extern "C" {
+
+int orc_nvar(void) { return NV; }
+int orc_real_size(void) { return (int)sizeof(R); }
+int orc_is_reference(void) { return 1; }
+
+int orc_set_para(const char *key, double val)
+{
+  for (auto &k : keys)
+    if (!std::strcmp(k.name, key)) { *k.val = (R)val; return 0; }
+  return -1;
+}
+double orc_get_para(const char *key)
+{
+  for (auto &k : keys)
+    if (!std::strcmp(k.name, key)) return (double)*k.val;
+  return NAN;
+}
+void orc_set_delta(double a, double b) { Delta1 = (R)a; Delta2 = (R)b; }
+void orc_set_rand(double r1, double r2)
+{
+#if defined(FG2_SCHEME_ISOT)
+  rand1 = (R)r1; rand2 = (R)r2;
+#else
+  (void)r1; (void)r2;
+#endif
+}
+
+int orc_threads(int n)
+{
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+void orc_kick(R *v, const R *u, int n1, int n2, double t, double beta) { orc::kick(v, u, n1, n2, (R)t, (R)beta); }
+int orc_drift(R *u, const R *v, int n1, int n2, double dt) { return orc::drift(u, v, n1, n2, (R)dt); }
+void orc_bcond(R *u, int n1, int n2, int p1, int p2) { orc::bcond(u, n1, n2, p1, p2); }
+void orc_euler(R *u, int n1, int n2, double dt) { orc::euler(u, n1, n2, (R)dt); }
+int orc_step(R *u, R *v, int n1, int n2, double t, double dt, int p1, int p2)
+{
+  return orc::step(u, v, n1, n2, (E)t, (E)dt, p1, p2);
+}
+int orc_run(R *u, R *v, int n1, int n2, double t, double dt, int nsteps, int p1, int p2)
+{
+  int nan = 0;
+  E tt = t;
+  for (int n = 0; n < nsteps; ++n) {
+    nan |= orc::step(u, v, n1, n2, tt, (E)dt, p1, p2);
+    tt += dt;
+  }
+  return nan;
+}
+
+// The reference's derivative macros evaluated at every interior cell (field by index).
+void orc_deriv(const R *u, int n1, int n2, int which, int field, R *out)
+{
+  const int s = orc::pitch(n2);
+  const S *o = (const S *)(u + orc::H * (s + NV));
+  const int sc = s / NV;
+  for (int i = 0; i < n1; ++i)
+    for (int j = 0; j < n2; ++j) {
+      const S *u = o + (long)i * sc + j;  // THIS = u, STRIDE = s (src/deriv.h:25-31)
+      const int s = sc;
+      R r = 0, fld[5][NVAR];
+      fld[0][0] = D1(lnd); fld[0][1] = D1(u1); fld[0][2] = D1(u2);
+      fld[1][0] = D2(lnd); fld[1][1] = D2(u1); fld[1][2] = D2(u2);
+      fld[2][0] = D11(lnd); fld[2][1] = D11(u1); fld[2][2] = D11(u2);
+      fld[3][0] = D22(lnd); fld[3][1] = D22(u1); fld[3][2] = D22(u2);
+      fld[4][0] = D12(lnd); fld[4][1] = D12(u1); fld[4][2] = D12(u2);
+#if defined(FG2_SCHEME_HYDRO)
+      fld[0][3] = D1(lne); fld[1][3] = D2(lne); fld[2][3] = D11(lne); fld[3][3] = D22(lne);
+      fld[4][3] = D12(lne);
+#endif
+      r = fld[which][field];
+      out[(long)i * n2 + j] = r;
+    }
+}
+
+}  // extern "C"

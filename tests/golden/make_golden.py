@@ -1,0 +1,129 @@
+"""Generate the golden vectors in tests/golden/*.npz from the REFERENCE's own arithmetic.
+
+Runs only where the reference tree is present (it builds oracle/_ref/ from it): the
+reference's src/deriv.h and src/<scheme>/eqns.cuh, Euler.cuh and bcond.cuh compiled for
+the host by oracle/ref_harness.cpp, driven by the loops of oracle/loops.h that follow
+src/step.cpp, src/kick.cu, src/drift.cu and src/bcond.cu.  The fixtures then travel
+with the repository; tests read them, never the reference.
+
+    python tests/golden/make_golden.py        (rebuilds oracle/, rewrites the fixtures)
+
+Every case stores its inputs, parameters and outputs, so a test needs nothing else.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from oracle.oracle import Oracle, default_box, reference_delta, reference_dt  # noqa: E402
+
+
+def noise_state(rng, n1, n2, nv, sigma=0.01, lne=np.log(0.9)):
+    x = np.zeros((n1, n2, nv))
+    x[..., 1:3] = rng.normal(0.0, sigma, (n1, n2, 2))
+    if nv == 4:
+        x[..., 3] = lne
+    return x
+
+
+def shear_state(rng, n1, n2, nv, gamma=5.0 / 3.0):
+    """A small tanh shear layer with density contrast (the shape of the large-grid case)."""
+    x1 = (np.arange(n1) + 0.5) / n1
+    x2 = (np.arange(n2) + 0.5) / n2
+    X, Y = np.meshgrid(x1, x2, indexing="ij")
+    inside = np.abs(Y - 0.5) < 0.25
+    rho = np.where(inside, 1.0, 2.0)
+    ux = 0.5 * np.tanh((np.abs(Y - 0.5) - 0.25) / 0.05)
+    uy = 0.01 * np.sin(4 * np.pi * X) + rng.normal(0, 1e-4, X.shape)
+    x = np.zeros((n1, n2, nv))
+    x[..., 0] = np.log(rho)
+    x[..., 1] = ux
+    x[..., 2] = uy
+    if nv == 4:
+        x[..., 3] = np.log(2.5 / (rho * (gamma - 1.0)))
+    return x
+
+
+CASES = [
+    # name, scheme, prec, n1, n2, init, para, steps, p1, p2, euler rand
+    ("hydro_noise_f32", "hydro", "f32", 24, 32, "noise", {}, 10, 1, 1, None),
+    ("hydro_noise_f64", "hydro", "f64", 24, 32, "noise", {}, 10, 1, 1, None),
+    ("hydro_shear_odd_f32", "hydro", "f32", 19, 37, "shear", {"dd": 1e-3}, 10, 1, 1, None),
+    ("hydro_nub_f32", "hydro", "f32", 16, 24, "noise", {"nub": 1e-3, "gamma": 1.4, "kappa": 1e-3}, 10, 1, 1, None),
+    ("hydro_walls_f32", "hydro", "f32", 20, 28, "shear", {}, 10, 0, 0, None),
+    ("isot_noise_f32", "hydro-isot", "f32", 24, 32, "noise", {}, 10, 1, 1, None),
+    ("isot_noise_f64", "hydro-isot", "f64", 24, 32, "noise", {}, 10, 1, 1, None),
+    ("isot_kolmogorov_f32", "hydro-isot", "f32", 20, 24, "noise", {"f": 0.05, "k": -2, "dd": 1e-3}, 10, 1, 1, None),
+    ("isot_forced_f32", "hydro-isot", "f32", 16, 20, "noise", {"f": 0.05, "k": 2}, 5, 1, 1, (1.234, 4.321)),
+    ("isot_walls_f32", "hydro-isot", "f32", 18, 22, "noise", {}, 10, 0, 0, None),
+]
+
+
+def make_case(name, scheme, prec, n1, n2, init, para, steps, p1, p2, rand, seed):
+    o = Oracle(scheme, prec, "reference")
+    rng = np.random.default_rng(seed)
+    l1, l2 = default_box(scheme)
+    if prec == "f32":  # Delta and getdt() in R = float (src/config.cpp:39, src/getdt.cpp:26)
+        d1, d2 = reference_delta(n1, n2, l1, l2)
+        dt = reference_dt(n1, n2, l1, l2)
+    else:  # R = double
+        d1, d2 = l1 / n1, l2 / n2
+        dt = 0.5 / (n1 / l1 + n2 / l2)
+    o.set_delta(d1, d2)
+    for k, val in para.items():
+        o.set_para(k, val)
+    x0 = noise_state(rng, n1, n2, o.nvar) if init == "noise" else shear_state(rng, n1, n2, o.nvar)
+    x0 = x0.astype(o.dtype)
+
+    # one kick from the initial state (v = F(u) at beta = 0, then beta != 0 on a known v)
+    u = o.padded(x0)
+    o.bcond(u, p1, p2)
+    v = o.empty(n1, n2)
+    o.kick(v, u, 0.0, 0.0)
+    f0 = o.interior(v).copy()
+    v_in = rng.normal(0, 1.0, (n1, n2, o.nvar)).astype(o.dtype)
+    v = o.padded(v_in)
+    o.kick(v, u, 0.0, -5.0 / 9.0)
+    f1 = o.interior(v).copy()
+
+    # `steps` full RK3 steps at the reference's fixed dt
+    u = o.padded(x0)
+    v = o.empty(n1, n2)
+    if rand is not None:
+        o.set_rand(*rand)
+    nan = 0
+    t = 0.0
+    for _ in range(steps):
+        nan |= o.step(u, v, t, dt, p1, p2)
+        t += dt
+    # reset parameters for the next case (the harness keeps them in globals)
+    defaults = {"hydro": {"gamma": 5 / 3, "nus": 2e-4, "nub": 0.0, "kappa": 5e-4, "dd": 0.0},
+                "hydro-isot": {"dd": 0.0, "nus": 2e-4, "nub": 0.0, "cs2": 1.0, "f": 0.0, "k": -8.0}}[scheme]
+    for k, val in defaults.items():
+        o.set_para(k, val)
+    return dict(
+        scheme=scheme, prec=prec, n1=n1, n2=n2, p1=p1, p2=p2, steps=steps, dt=dt,
+        l1=l1, l2=l2, delta1=d1, delta2=d2,
+        para_keys=np.array(list(para.keys()), dtype="U16"),
+        para_vals=np.array(list(para.values()), dtype=np.float64),
+        rand=np.array(rand if rand is not None else (0.0, 0.0)), has_rand=rand is not None,
+        x0=x0, v_in=v_in, kick0=f0, kick1=f1, out=o.interior(u).copy(), nan=nan,
+    )
+
+
+def main():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    for seed, case in enumerate(CASES, start=1):
+        d = make_case(*case, seed=seed)
+        path = os.path.join(HERE, case[0] + ".npz")
+        np.savez_compressed(path, seed=seed, **d)
+        print(f"{case[0]:24s} {os.path.getsize(path):7d} B  nan={d['nan']}  "
+              f"|out|max={np.abs(d['out']).max():.4g}")
+
+
+if __name__ == "__main__":
+    main()

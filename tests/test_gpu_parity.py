@@ -1,0 +1,220 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's arithmetic: the
+committed golden vectors (made by the reference's own headers compiled for the host) and
+the CPU port on seeded inputs.  Tolerance: per-field relative L2 <= 1e-5 after 10 steps in
+FP32 (the documented bar), <= 1e-12 in FP64."""
+import numpy as np
+import pytest
+
+import fg2_b200
+from helpers import golden_cases, load_golden, rel_l2
+from oracle.oracle import Oracle, reference_delta, reference_dt
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f32": 1e-5, "f64": 1e-12}
+
+
+def sim_for(g):
+    sim = fg2_b200.Sim(g["n1"], g["n2"], scheme=g["scheme"], storage=g["prec"])
+    sim.set_bcond(g["p1"], g["p2"])
+    for k, v in g["para"].items():
+        assert sim.para(f"{k}={v!r}") is not None
+    sim.config()
+    if g["has_rand"]:
+        sim.set_forcing_phases(*g["rand"])
+    sim.upload(g["x0"])
+    return sim
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_steps_match_golden(name, cuda):
+    g = load_golden(name)
+    with sim_for(g) as sim:
+        t = 0.0
+        for _ in range(g["steps"]):
+            assert sim.step(t, g["dt"]) == 0
+            t += g["dt"]
+        out = sim.download()
+    err = rel_l2(out, g["out"])
+    assert np.all(err <= TOL[g["prec"]]), (name, err)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_kick_matches_golden(name, cuda):
+    g = load_golden(name)
+    with sim_for(g) as sim:
+        sim.bcond()
+        sim.kick(0.0, 0.0)
+        f0 = sim.download_v()
+        sim.upload_v(g["v_in"])
+        sim.kick(0.0, -5.0 / 9.0)
+        f1 = sim.download_v()
+    assert np.all(rel_l2(f0, g["kick0"]) <= TOL[g["prec"]] * 0.1)
+    assert np.all(rel_l2(f1, g["kick1"]) <= TOL[g["prec"]] * 0.1)
+
+
+@pytest.mark.parametrize("scheme,n1,n2", [("hydro", 256, 256), ("hydro", 37, 53), ("hydro", 64, 7),
+                                          ("hydro", 130, 67), ("hydro-isot", 96, 160), ("hydro-isot", 5, 9)])
+def test_port_parity_seeded(scheme, n1, n2, cuda):
+    """The small plain configuration (256^2, Gaussian velocity noise, fixed dt) and ragged
+    sizes: 10 GPU steps against 10 oracle steps from the same seeded state."""
+    o = Oracle(scheme, "f32", "port")
+    with fg2_b200.Sim(n1, n2, scheme=scheme) as sim:
+        sim.config()
+        sim.init("noise", seed=1)
+        x0 = sim.download()
+        l = (1.0, 1.0) if scheme == "hydro" else (2 * np.pi, 2 * np.pi)
+        dt = reference_dt(n1, n2, *l)
+        assert sim.getdt() == dt
+        for n in range(10):
+            assert sim.step(n * dt, dt) == 0
+        gpu = sim.download()
+    o.set_delta(*reference_delta(n1, n2, *l))
+    u = o.padded(x0)
+    v = o.empty(n1, n2)
+    assert o.run(u, v, 0.0, dt, 10) == 0
+    err = rel_l2(gpu, o.interior(u))
+    assert np.all(err <= 1e-5), err
+
+
+def test_fused_step_equals_reference_building_blocks(cuda):
+    """step() == Euler + 3 x (bcond, kick, drift) through the separate entry points."""
+    n1, n2 = 48, 40
+    coef = [(0.0, 1.0 / 3.0), (-5.0 / 9.0, 15.0 / 16.0), (-153.0 / 128.0, 8.0 / 15.0)]
+    with fg2_b200.Sim(n1, n2) as a, fg2_b200.Sim(n1, n2) as b:
+        for s in (a, b):
+            s.config()
+            s.init("kh", seed=3)
+        dt = a.getdt()
+        assert a.step(0.0, dt) == 0
+        for beta, gamma in coef:
+            b.bcond()
+            b.kick(0.0, beta)
+            assert b.drift(float(np.float32(dt * gamma))) == 0
+        ua, ub = a.download(), b.download()
+    assert np.array_equal(ua, ub) or np.all(rel_l2(ua, ub) < 1e-7)
+
+
+def test_graph_replay_is_bit_identical(cuda):
+    with fg2_b200.Sim(96, 128) as a, fg2_b200.Sim(96, 128) as b:
+        for s in (a, b):
+            s.config()
+            s.init("noise", seed=9)
+        dt = a.getdt()
+        a.advance(6, dt)
+        b.advance(6, dt, graph=True)
+        assert a.sync() == 0 and b.sync() == 0
+        assert np.array_equal(a.download(), b.download())
+
+
+def test_cfl_getdt_matches_host_reduction(cuda):
+    n1, n2 = 64, 80
+    with fg2_b200.Sim(n1, n2) as s:
+        s.config()
+        s.init("kh", seed=4)
+        s.set_dt_mode("cfl")
+        dt = s.getdt()
+        q = s.download().astype(np.float64)
+    gamma = float(np.float32(5 / 3))
+    cs = np.sqrt(gamma * (gamma - 1) * np.exp(q[..., 3]))
+    d1, d2 = reference_delta(n1, n2, 1.0, 1.0)
+    rate = ((np.abs(q[..., 1]) + cs) / d1 + (np.abs(q[..., 2]) + cs) / d2).max()
+    D = max(4 / 3 * float(np.float32(2e-4)), (gamma - 1) * float(np.float32(5e-4)))
+    dt_diff = 0.5 * 2.51 / (D * 1088 / 180 * (1 / d1 ** 2 + 1 / d2 ** 2))
+    assert dt == pytest.approx(min(0.5 / rate, dt_diff), rel=1e-12)
+
+
+def test_device_resident_dt_tracks_host_loop(cuda):
+    """advance(dt <= 0): getdt fused into the last stage, dt and t kept on the device."""
+    n1, n2, nsteps = 64, 64, 8
+    with fg2_b200.Sim(n1, n2) as a, fg2_b200.Sim(n1, n2) as b:
+        for s in (a, b):
+            s.config()
+            s.init("kh", seed=5)
+            s.set_dt_mode("cfl")
+        t = 0.0
+        for _ in range(nsteps):
+            dt = a.getdt()
+            assert a.step(t, dt) == 0
+            t += dt
+        b.set_time(0.0)
+        b.advance(nsteps, 0.0, graph=True)
+        assert b.sync() == 0
+        assert b.time() == pytest.approx(t, rel=1e-6)
+        assert np.all(rel_l2(b.download(), a.download()) < 1e-5)
+
+
+def test_t_end_caps_the_device_clock(cuda):
+    with fg2_b200.Sim(32, 32) as s:
+        s.config()
+        s.init("noise", seed=1)
+        s.set_time(0.0)
+        s.advance(20, 0.0, t_end=1e-3)
+        assert s.sync() == 0
+        assert s.time() == pytest.approx(1e-3, rel=1e-12)
+
+
+def test_nan_in_the_input_is_reported(cuda):
+    with fg2_b200.Sim(32, 48) as s:
+        s.config()
+        s.init("noise", seed=1)
+        x = s.download()
+        x[10, 11, 1] = np.nan
+        s.upload(x)
+        assert s.step(0.0, 1e-3) == 1  # cudaErrorInvalidValue, src/step.cpp:38-40
+
+
+def test_sums_are_reproducible_fp64(cuda):
+    with fg2_b200.Sim(200, 160) as s:
+        s.config()
+        s.init("kh", seed=2)
+        a, b = s.sums(), s.sums()
+        q = s.download().astype(np.float64)
+    assert np.array_equal(a, b)
+    rho = np.exp(q[..., 0])
+    ref = [rho.sum(), (rho * q[..., 1]).sum(), (rho * q[..., 2]).sum(),
+           (rho * (np.exp(q[..., 3]) + 0.5 * (q[..., 1] ** 2 + q[..., 2] ** 2))).sum()]
+    np.testing.assert_allclose(a, ref, rtol=1e-12, atol=1e-9)
+
+
+def test_raw_frame_round_trip(cuda, tmp_path):
+    path = tmp_path / "0001.raw"
+    with fg2_b200.Sim(40, 56) as s:
+        s.config()
+        s.init("turb", seed=7)
+        s.dump(path, 0.25)
+        x = s.download()
+    raw = np.fromfile(path, dtype=np.uint8)
+    hdr = np.frombuffer(raw[:24].tobytes(), np.int32)
+    assert list(hdr) == [40, 56, 4, 4, 1, 1]  # n1, n2, NVAR, sizeof(R), p1, p2 (src/io.cpp:62)
+    assert np.frombuffer(raw[24:32].tobytes(), np.float64)[0] == 0.25
+    data = np.frombuffer(raw[44:].tobytes(), np.float32).reshape(40, 56, 4)
+    assert np.array_equal(data, x)
+    with fg2_b200.Sim(40, 56) as s:
+        assert s.load(path) == 0.25
+        assert np.array_equal(s.download(), x)
+
+
+def test_reference_mirror_api(cuda):
+    """fg2_setup / fg2_para / fg2_config / fg2_init / fg2_getdt / fg2_step, the function
+    contract of src/fg2.h:70-84, give what the handle API gives."""
+    lib = fg2_b200.load_library("hydro")
+    assert lib.fg2_setup(64, 48) > 0
+    assert lib.fg2_para(b"--nus=3e-4") == b"nus = 0.0003"
+    assert lib.fg2_para(b"nosuchkey=1") is None
+    lib.fg2_config()
+    lib.fg2_init(b"noise")
+    dt = lib.fg2_getdt()
+    for n in range(3):
+        assert lib.fg2_step(n * dt, dt) == 0
+    g = fg2_b200.Sim.__new__(fg2_b200.Sim)
+    g.lib, g.h, g.n1, g.n2, g.nvar, g.host_dtype = lib, lib.fg2_global(), 64, 48, 4, np.float32
+    ug = g.download()
+    g.h = None  # not owned
+    with fg2_b200.Sim(64, 48) as s:
+        s.para("nus=3e-4")
+        s.config()
+        s.init("noise", seed=0)
+        for n in range(3):
+            assert s.step(n * dt, dt) == 0
+        assert np.array_equal(s.download(), ug)
