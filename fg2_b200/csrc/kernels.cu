@@ -167,7 +167,10 @@ __global__ void __launch_bounds__(NT) substage_kernel(const __grid_constant__ CU
     // padded coordinates: column j0 - 4 + GL = j0, row i0 - 3 + GT = i0, all fields
     tma_load_3d(tile, &tm, bar, j0, i0, 0);
   }
-  if (!mbar_wait_bounded(bar, 0, WAIT_NS)) {
+  // every thread waits (bounded); the CTA then agrees on the outcome so that all threads
+  // take the same path through the warp-collective epilogue
+  const bool landed = mbar_wait_bounded(bar, 0, WAIT_NS);
+  if (__syncthreads_or(!landed)) {
     if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
     mbar_wait_bounded(bar, 0, WAIT_NS);  // let the copy in flight land before exiting
     return;

@@ -39,8 +39,27 @@ def test_steps_match_golden(name, cuda):
     assert np.all(err <= TOL[g["prec"]]), (name, err)
 
 
+def f64_kick(g, v_in=None, beta=0.0):
+    """The right-hand side in FP64 (the port at R = double) from the same FP32 inputs."""
+    o = Oracle(g["scheme"], "f64", "port")
+    defaults = {"hydro": {"gamma": 5 / 3, "nus": 2e-4, "nub": 0.0, "kappa": 5e-4, "dd": 0.0},
+                "hydro-isot": {"dd": 0.0, "nus": 2e-4, "nub": 0.0, "cs2": 1.0, "f": 0.0, "k": -8.0}}[g["scheme"]]
+    for k, v in {**defaults, **g["para"]}.items():
+        o.set_para(k, float(np.float32(v)) if g["prec"] == "f32" else v)
+    o.set_delta(g["delta1"], g["delta2"])
+    u = o.padded(g["x0"].astype(np.float64))
+    o.bcond(u, g["p1"], g["p2"])
+    v = o.empty(g["n1"], g["n2"]) if v_in is None else o.padded(v_in.astype(np.float64))
+    o.kick(v, u, 0.0, beta)
+    return o.interior(v).copy()
+
+
 @pytest.mark.parametrize("name", golden_cases())
 def test_kick_matches_golden(name, cuda):
+    """One right-hand-side evaluation.  Its fields can be small differences of large terms
+    (the pressure gradient of a pressure-balanced shear layer nearly cancels), so besides
+    the golden comparison the GPU's rounding error against FP64 must stay within three times
+    the reference's own FP32 rounding error, or 5e-6 (about 80 FP32 ulps), whichever is larger."""
     g = load_golden(name)
     with sim_for(g) as sim:
         sim.bcond()
@@ -49,8 +68,12 @@ def test_kick_matches_golden(name, cuda):
         sim.upload_v(g["v_in"])
         sim.kick(0.0, -5.0 / 9.0)
         f1 = sim.download_v()
-    assert np.all(rel_l2(f0, g["kick0"]) <= TOL[g["prec"]] * 0.1)
-    assert np.all(rel_l2(f1, g["kick1"]) <= TOL[g["prec"]] * 0.1)
+    tol = 1e-4 if g["prec"] == "f32" else 1e-12
+    assert np.all(rel_l2(f0, g["kick0"]) <= tol), rel_l2(f0, g["kick0"])
+    assert np.all(rel_l2(f1, g["kick1"]) <= tol), rel_l2(f1, g["kick1"])
+    if g["prec"] == "f32":
+        truth = f64_kick(g)
+        assert np.all(rel_l2(f0, truth) <= np.maximum(3 * rel_l2(g["kick0"], truth), 5e-6))
 
 
 @pytest.mark.parametrize("scheme,n1,n2", [("hydro", 256, 256), ("hydro", 37, 53), ("hydro", 64, 7),
