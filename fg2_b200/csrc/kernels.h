@@ -9,6 +9,9 @@
 
 namespace fg2 {
 
+// Records the text of the last library error (read back by fg2_last_error) and returns code.
+int set_error(int code, const char *fmt, ...);
+
 // Scalar inputs of one substage launch (RK3 stage s: v <- F(u) + beta v,
 // u_out <- u + gamma dt v), all in the host's double precision; each launcher rounds them
 // to the compute type the way the reference rounds E-precision coefficients to R.

@@ -32,10 +32,10 @@
 using namespace fg2;
 
 namespace {
-
 thread_local char g_err[512] = "";
+}  // namespace
 
-int fail(int code, const char *fmt, ...)
+int fg2::set_error(int code, const char *fmt, ...)
 {
   va_list ap;
   va_start(ap, fmt);
@@ -43,6 +43,10 @@ int fail(int code, const char *fmt, ...)
   va_end(ap);
   return code;
 }
+
+namespace {
+
+#define fail fg2::set_error
 
 int cuda_status(cudaError_t e, const char *what)
 {

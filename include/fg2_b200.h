@@ -134,6 +134,21 @@ void *fg2_sim_stream(fg2_sim *s);
 int fg2_sim_dump(fg2_sim *s, const char *path, double time);
 int fg2_sim_load(fg2_sim *s, const char *path, double *time);
 
+/* ---- allocation-free sums ---------------------------------------------------------------
+ * No counterpart in the reference.  The FP64 sums of fg2_sim_sums for callers that cannot
+ * call cudaMalloc (their allocator already holds the GPU's memory, or the call sits in a
+ * loop that must not allocate, or they hold a state array but no handle).  The caller
+ * passes the state array u (device memory in the layout of fg2_sim_layout, storage FG2_F32
+ * or FG2_F64) and out, a device buffer of 4 doubles.  The only scratch is a static device
+ * array of FG2_NOALLOC_MAX_ROWS x 4 doubles (512 KiB) that every GPU loading this library
+ * holds until the process exits; grids with more rows are rejected with FG2_ERR_ARG.  All
+ * calls share that array, so calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's device address; make it before any stream capture.
+ * Enqueued on `stream` without synchronising. */
+#define FG2_NOALLOC_MAX_ROWS 16384
+int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, long long plane, int storage, double *out,
+                     void *stream);
+
 /* ---- reference-mirror API (src/fg2.h:60-84) over one process-wide simulation ------------ */
 size_t fg2_setup(int n1, int n2);          /* bytes of device memory, 0 on failure */
 void fg2_config(void);
