@@ -1,19 +1,24 @@
 // fg2_b200/csrc/fg2b.h -- shared host/device definitions of the B200 time-step library.
 //
-// Device layout of one simulation (structure of arrays, one plane per field):
-//   element (f, i, j), i in [-3, n1+3), j in [-4, n2+4), lives at
-//       base[f * PS + (i + GT) * P + (j + GL)]
+// Device layout of one simulation (rows of field segments): element (f, i, j),
+// i in [-3, n1+3), j in [-4, n2+4), lives at
+//       base[f * FS + (i + GT) * RS + (j + GL)]
 //   GT = 3 ghost rows above/below (HALF of the 6th-order stencil, src/fg2.h:26-34);
 //   GL = 4 columns left of the interior: 3 ghosts plus one so that the interior and every
 //   tile's halo start on a 16-byte boundary (a TMA box must start on one);
-//   P  = row pitch, >= n2 + 8, rounded up so rows start on 128 bytes;
-//   PS = (n1 + 6) * P, the plane stride.
+//   FS = field stride = P >= n2 + 8, rounded up so every field row starts on 128 bytes;
+//   RS = row stride = NVAR * P (the NVAR field rows of grid row i are consecutive).
 // Axis 1 (i, n1, Delta1) is the slow, strided axis and axis 2 (j, n2, Delta2) the
 // contiguous one, as in the reference (src/deriv.h:33, src/init.cpp:31-35).
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <vector_types.h>
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#endif
 
 #if defined(__CUDACC__)
 #define FG2_HD __host__ __device__ __forceinline__
@@ -36,19 +41,20 @@ enum Bc : int { BC_WALL = 0, BC_PERIODIC = 1 };
 
 struct Layout {
   int n1, n2;
-  long long P;   // row pitch, elements
-  long long PS;  // plane stride, elements
-  FG2_HD long long at(int f, int i, int j) const { return f * PS + (long long)(i + GT) * P + (j + GL); }
+  long long RS;  // row stride, elements
+  long long FS;  // field stride, elements
+  FG2_HD long long at(int f, int i, int j) const { return f * FS + (long long)(i + GT) * RS + (j + GL); }
+  FG2_HD long long elems() const { return (long long)(n1 + 2 * GT) * RS; }
 };
 
-inline Layout make_layout(int n1, int n2, size_t elem)
+inline Layout make_layout(int n1, int n2, int nvar, size_t elem)
 {
   Layout L;
   L.n1 = n1;
   L.n2 = n2;
   const long long align = 128 / (long long)elem;
-  L.P = ((long long)n2 + 2 * GL + align - 1) / align * align;
-  L.PS = (long long)(n1 + 2 * GT) * L.P;
+  L.FS = ((long long)n2 + 2 * GL + align - 1) / align * align;
+  L.RS = nvar * L.FS;
   return L;
 }
 
@@ -60,6 +66,7 @@ struct Coef {
   C a1[3], a2[3];      // first derivative weights, axis 1 / axis 2, k = 1..3
   C b1[4], b2[4];      // second derivative weights (centre, k = 1..3)
   C m[3];              // mixed derivative weights
+  C mn[3];             // their negatives
   C delta1, delta2;    // grid spacings (the reference's Delta1/Delta2, rounded to C)
   C inv1, inv2;        // 1 / Delta
 };
@@ -83,10 +90,12 @@ struct ParaKey {
   double def;
 };
 
-// Per-launch scalar parameters of a scheme, by slot (at most 8 keys per scheme).
+// Per-launch parameters of a scheme, by slot: the runtime keys first, then constants the
+// scheme derives from them on the host (scheme::derive), at most NPARA in all.
+constexpr int NPARA = 12;
 template <class C>
 struct Para {
-  C v[8];
+  C v[NPARA];
 };
 
 // Status block shared by the kernels and the host (device memory, one per simulation).
@@ -100,5 +109,92 @@ struct Status {
   unsigned long long steps;     // steps taken by device-resident runs
 };
 enum ErrorBits : unsigned { ERR_TMA_TIMEOUT = 1u, ERR_QUEUE_TIMEOUT = 2u };
+
+// ---- arithmetic on a scalar or on a pair of cells ------------------------------------------
+// The fused kernel evaluates two cells per thread; for FP32 the pair is a float2 and every
+// operation is one packed sm_100 instruction (add/mul/fma .f32x2), for FP64 a double2
+// evaluated component-wise.  Scheme code is written once against these helpers.
+template <class C>
+struct Scalar {
+  using type = C;
+};
+template <>
+struct Scalar<float2> {
+  using type = float;
+};
+template <>
+struct Scalar<double2> {
+  using type = double;
+};
+
+template <class C>
+FG2_HD C lit(double x) { return (C)x; }
+template <class C>
+FG2_HD typename Scalar<C>::type first(C x) { return x; }
+FG2_HD float fmac(float a, float b, float c) { return fmaf(a, b, c); }
+FG2_HD double fmac(double a, double b, double c) { return fma(a, b, c); }
+
+template <>
+FG2_HD float2 lit<float2>(double x) { return make_float2((float)x, (float)x); }
+template <>
+FG2_HD double2 lit<double2>(double x) { return make_double2(x, x); }
+template <>
+FG2_HD float first<float2>(float2 x) { return x.x; }
+template <>
+FG2_HD double first<double2>(double2 x) { return x.x; }
+
+}  // namespace fg2
+
+// Pair arithmetic, in the global namespace like float2 and double2 themselves so that
+// argument-dependent lookup finds it from scheme code.
+#if defined(__CUDACC__)
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 &operator+=(float2 &a, float2 b) { return a = a + b; }
+__device__ __forceinline__ float2 &operator-=(float2 &a, float2 b) { return a = a - b; }
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 operator*(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 operator-(double2 a) { return make_double2(-a.x, -a.y); }
+__device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 &operator+=(double2 &a, double2 b) { return a = a + b; }
+__device__ __forceinline__ double2 &operator-=(double2 &a, double2 b) { return a = a - b; }
+#endif
+
+namespace fg2 {
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ float2 fmac(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float2 vexp(float2 a) { return make_float2(__expf(a.x), __expf(a.y)); }
+__device__ __forceinline__ float2 vsqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
+__device__ __forceinline__ float2 vmax(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+__device__ __forceinline__ float2 vcos(float2 a) { return make_float2(cosf(a.x), cosf(a.y)); }
+__device__ __forceinline__ double2 fmac(double2 a, double2 b, double2 c)
+{
+  return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 vabs(double2 a) { return make_double2(fabs(a.x), fabs(a.y)); }
+__device__ __forceinline__ double2 vexp(double2 a) { return make_double2(exp(a.x), exp(a.y)); }
+__device__ __forceinline__ double2 vsqrt(double2 a) { return make_double2(sqrt(a.x), sqrt(a.y)); }
+__device__ __forceinline__ double2 vmax(double2 a, double2 b) { return make_double2(fmax(a.x, b.x), fmax(a.y, b.y)); }
+__device__ __forceinline__ double2 vcos(double2 a) { return make_double2(cos(a.x), cos(a.y)); }
+#endif
+
+FG2_HD float vabs(float a) { return fabsf(a); }
+FG2_HD double vabs(double a) { return fabs(a); }
+FG2_HD float vsqrt(float a) { return sqrtf(a); }
+FG2_HD double vsqrt(double a) { return sqrt(a); }
+FG2_HD float vmax(float a, float b) { return fmaxf(a, b); }
+FG2_HD double vmax(double a, double b) { return fmax(a, b); }
+FG2_HD double vexp(double a) { return exp(a); }
+FG2_HD float vcos(float a) { return cosf(a); }
+FG2_HD double vcos(double a) { return cos(a); }
+#if defined(__CUDACC__)
+__device__ __forceinline__ float vexp(float a) { return __expf(a); }
+#else
+inline float vexp(float a) { return expf(a); }
+#endif
 
 }  // namespace fg2

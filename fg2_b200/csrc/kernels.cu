@@ -33,22 +33,44 @@ constexpr int NV = scheme::NVAR;
 constexpr uint64_t WAIT_NS = 2000000000ull;  // bound of every in-kernel wait (2 s)
 
 // ---------------------------------------------------------------------------------------
-// Parameters rounded to the compute type C.
-template <class C>
+// Two cells per thread: the pair type of a storage type (packed FP32x2 for float).
+template <class T>
+struct PairOf;
+template <>
+struct PairOf<float> {
+  using type = float2;
+  static __host__ __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
+};
+template <>
+struct PairOf<double> {
+  using type = double2;
+  static __host__ __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+};
+
+// Parameters of one substage launch, rounded to the storage precision T and broadcast to
+// both lanes of a pair (so packed instructions read them straight from the constant bank).
+template <class T>
 struct KParams {
-  Coef<C> k;
-  Para<C> p;
-  C beta;
+  using P = typename PairOf<T>::type;
+  Coef<P> k;
+  Para<P> p;
+  P beta;
   double gamma, dt;
   const double *dt_dev;
   int p1, p2;
   Status *status;
 };
 
-template <class C>
-static KParams<C> make_params(const StageArgs &a)
+template <class T>
+static typename PairOf<T>::type bc(double x)
 {
-  KParams<C> kp;
+  return PairOf<T>::make((T)x, (T)x);
+}
+
+template <class T>
+static KParams<T> make_params(const StageArgs &a)
+{
+  KParams<T> kp;
   // Delta = l / n is rounded to the state precision (src/config.cpp:39); the weights are
   // divided by it in double and rounded once.
   const double d1 = a.delta1, d2 = a.delta2;
@@ -56,20 +78,21 @@ static KParams<C> make_params(const StageArgs &a)
   const double w2[4] = {-490. / 180., 270. / 180., -27. / 180., 2. / 180.};
   const double wm[3] = {270. / 720., -27. / 720., 2. / 720.};
   for (int q = 0; q < 3; ++q) {
-    kp.k.a1[q] = (C)(w1[q] / d1);
-    kp.k.a2[q] = (C)(w1[q] / d2);
-    kp.k.m[q] = (C)(wm[q] / (d1 * d2));
+    kp.k.a1[q] = bc<T>(w1[q] / d1);
+    kp.k.a2[q] = bc<T>(w1[q] / d2);
+    kp.k.m[q] = bc<T>(wm[q] / (d1 * d2));
+    kp.k.mn[q] = bc<T>(-wm[q] / (d1 * d2));
   }
   for (int q = 0; q < 4; ++q) {
-    kp.k.b1[q] = (C)(w2[q] / (d1 * d1));
-    kp.k.b2[q] = (C)(w2[q] / (d2 * d2));
+    kp.k.b1[q] = bc<T>(w2[q] / (d1 * d1));
+    kp.k.b2[q] = bc<T>(w2[q] / (d2 * d2));
   }
-  kp.k.delta1 = (C)d1;
-  kp.k.delta2 = (C)d2;
-  kp.k.inv1 = (C)(1.0 / d1);
-  kp.k.inv2 = (C)(1.0 / d2);
-  for (int q = 0; q < 8; ++q) kp.p.v[q] = (C)(a.para ? a.para[q] : 0.0);
-  kp.beta = (C)a.beta;
+  kp.k.delta1 = bc<T>(d1);
+  kp.k.delta2 = bc<T>(d2);
+  kp.k.inv1 = bc<T>(1.0 / d1);
+  kp.k.inv2 = bc<T>(1.0 / d2);
+  for (int q = 0; q < NPARA; ++q) kp.p.v[q] = bc<T>(a.para ? a.para[q] : 0.0);
+  kp.beta = bc<T>(a.beta);
   kp.gamma = a.gamma;
   kp.dt = a.dt;
   kp.dt_dev = a.dt_dev;
@@ -118,7 +141,7 @@ __device__ __forceinline__ void store_images(T *u, const Layout &L, int i, int j
     for (int b = 0; b < g.nc; ++b)
 #pragma unroll
       for (int f = 0; f < NV; ++f) {
-        const C x = g.flip[b] ? C(scheme::reflect_sign(f)) * q[f] : q[f];
+        const C x = (g.flip[b] && scheme::reflect_sign(f) < 0) ? -q[f] : q[f];
         u[L.at(f, g.rows[a], g.cols[b])] = (T)x;
       }
 }
@@ -127,198 +150,119 @@ template <class C>
 __device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, const Coef<C> &k)
 {
   const C cs = scheme::sound_speed(q, p);
-  return (fabs(q[scheme::U1]) + cs) * k.inv1 + (fabs(q[scheme::U2]) + cs) * k.inv2;
+  return fmac(vabs(q[scheme::U1]) + cs, k.inv1, (vabs(q[scheme::U2]) + cs) * k.inv2);
 }
+
+#include "substage.cuh"
 
 // ---------------------------------------------------------------------------------------
-// Fused substage.  One CTA per TW x TH tile; NT threads, TW columns x (NT / TW) row groups.
-template <class T, int TW, int TH, int NT>
-struct SubstageCfg {
-  static constexpr int BW = TW + 2 * GL;    // box width (columns j0-4 .. j0+TW+3)
-  static constexpr int BH = TH + 2 * HALF;  // box height (rows i0-3 .. i0+TH+2)
-  static constexpr int PLANE = BW * BH;
-  static constexpr size_t TILE_BYTES = (size_t)NV * PLANE * sizeof(T);
-  static constexpr size_t SMEM = TILE_BYTES + 16;
-  static_assert(BW <= 256 && BH <= 256, "TMA box dimensions are limited to 256");
-  static_assert((BW * sizeof(T)) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
-  static_assert(TILE_BYTES % 8 == 0, "mbarrier alignment");
-};
-
-template <class T, int TW, int TH, int NT, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
-__global__ void __launch_bounds__(NT) substage_kernel(const __grid_constant__ CUtensorMap tm, T *__restrict__ u_out,
-                                                      T *__restrict__ v, const Layout L, const KParams<T> a)
-{
-  using C = T;
-  using Cfg = SubstageCfg<T, TW, TH, NT>;
-  constexpr int BW = Cfg::BW, PLANE = Cfg::PLANE;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  T *tile = reinterpret_cast<T *>(smem_raw);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Cfg::TILE_BYTES);
-
-  const int i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
-  if (threadIdx.x == 0) {
-    prefetch_tmap(&tm);
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(bar, (uint32_t)Cfg::TILE_BYTES);
-    // padded coordinates: column j0 - 4 + GL = j0, row i0 - 3 + GT = i0, all fields
-    tma_load_3d(tile, &tm, bar, j0, i0, 0);
-  }
-  // every thread waits (bounded); the CTA then agrees on the outcome so that all threads
-  // take the same path through the warp-collective epilogue
-  const bool landed = mbar_wait_bounded(bar, 0, WAIT_NS);
-  if (__syncthreads_or(!landed)) {
-    if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-    mbar_wait_bounded(bar, 0, WAIT_NS);  // let the copy in flight land before exiting
-    return;
-  }
-
-  const C gdt = (C)(a.gamma * (a.dt_dev ? *a.dt_dev : a.dt));  // (R)(dt * gamma[i]), src/step.cpp:34
-  const unsigned m2 = scheme::d2_fields(a.p);
-  const int tx = threadIdx.x % TW, ty = threadIdx.x / TW;
-  constexpr int RG = NT / TW;
-  const int j = j0 + tx;
-  bool nan = false;
-  C rate = C(0);
-
-  for (int rr = ty; rr < TH; rr += RG) {
-    const int i = i0 + rr;
-    if (i >= L.n1 || j >= L.n2) continue;
-    const T *c0 = tile + (rr + HALF) * BW + (tx + GL);
-    Cell<C, NV> cell;
-#pragma unroll
-    for (int f = 0; f < NV; ++f) {
-      const T *c = c0 + f * PLANE;
-#define G(di, dj) ((C)c[(di) * BW + (dj)])
-      cell.q[f] = G(0, 0);
-      cell.d1[f] = a.k.a1[0] * (G(1, 0) - G(-1, 0)) + a.k.a1[1] * (G(2, 0) - G(-2, 0)) +
-                   a.k.a1[2] * (G(3, 0) - G(-3, 0));
-      cell.d2[f] = a.k.a2[0] * (G(0, 1) - G(0, -1)) + a.k.a2[1] * (G(0, 2) - G(0, -2)) +
-                   a.k.a2[2] * (G(0, 3) - G(0, -3));
-      if (m2 & (1u << f)) {
-        cell.d11[f] = a.k.b1[0] * G(0, 0) + a.k.b1[1] * (G(1, 0) + G(-1, 0)) + a.k.b1[2] * (G(2, 0) + G(-2, 0)) +
-                      a.k.b1[3] * (G(3, 0) + G(-3, 0));
-        cell.d22[f] = a.k.b2[0] * G(0, 0) + a.k.b2[1] * (G(0, 1) + G(0, -1)) + a.k.b2[2] * (G(0, 2) + G(0, -2)) +
-                      a.k.b2[3] * (G(0, 3) + G(0, -3));
-      } else {
-        cell.d11[f] = C(0);
-        cell.d22[f] = C(0);
-      }
-      if (scheme::D12_FIELDS & (1u << f)) {
-        cell.d12[f] = a.k.m[0] * (G(1, 1) - G(-1, 1) + G(-1, -1) - G(1, -1)) +
-                      a.k.m[1] * (G(2, 2) - G(-2, 2) + G(-2, -2) - G(2, -2)) +
-                      a.k.m[2] * (G(3, 3) - G(-3, 3) + G(-3, -3) - G(3, -3));
-      } else {
-        cell.d12[f] = C(0);
-      }
-#undef G
-    }
-    C r[NV];
-    scheme::eqns(cell, a.p, i, j, r, a.k.delta1);
-
-    const long long o = L.at(0, i, j);
-    C qn[NV];
-#pragma unroll
-    for (int f = 0; f < NV; ++f) {
-      C vn = r[f];
-      if (READ_V) vn = fma(a.beta, (C)v[o + f * L.PS], r[f]);
-      if (WRITE_V) v[o + f * L.PS] = (T)vn;
-      qn[f] = fma(gdt, vn, cell.q[f]);
-      nan |= qn[f] != qn[f];
-    }
-    if (WRITE_U) store_images<T, C>(u_out, L, i, j, qn, a.p1, a.p2);
-    if (CFL) rate = fmax(rate, cfl_rate<C>(qn, a.p, a.k));
-  }
-
-  if (WRITE_U) {
-    if (__any_sync(0xffffffffu, nan) && (threadIdx.x & 31) == 0) atomicOr(&a.status->nan, 1u);
-  }
-  if (CFL) {
-    double r = (double)rate;
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, s));
-    if ((threadIdx.x & 31) == 0 && r > 0.0)
-      atomicMax(&a.status->smax, (unsigned long long)__double_as_longlong(r));
-  }
-}
-
-// Tile shapes per storage type.
-constexpr int TW32 = 64, TH32 = 32, NT32 = 256;
-constexpr int TW64 = 64, TH64 = 32, NT64 = 256;
-
-TileShape substage_tile(int storage)
-{
-  if (storage == ST_F64) return {TW64, TH64, NT64, SubstageCfg<double, TW64, TH64, NT64>::SMEM};
-  return {TW32, TH32, NT32, SubstageCfg<float, TW32, TH32, NT32>::SMEM};
-}
-
-CUresult encode_state_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
+// Tensor maps: u with the halo box of one chunk, v with the interior box of one chunk.
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encoder()
 {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void *fn = nullptr;
     cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess || !fn)
-      return CUDA_ERROR_NOT_FOUND;
-    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
   }
-  const TileShape ts = substage_tile(storage);
+  return encode;
+}
+
+CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int storage, int box_w, int box_h)
+{
+  PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
+  if (!encode) return CUDA_ERROR_NOT_FOUND;
   const size_t elem = storage == ST_F64 ? 8 : (storage == ST_F32 ? 4 : 2);
   const CUtensorMapDataType dt = storage == ST_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                  : storage == ST_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : storage == ST_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                      : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  cuuint64_t dims[3] = {(cuuint64_t)(L.n2 + 2 * GL), (cuuint64_t)(L.n1 + 2 * GT), (cuuint64_t)NV};
-  cuuint64_t strides[2] = {(cuuint64_t)(L.P * elem), (cuuint64_t)(L.PS * elem)};
-  cuuint32_t box[3] = {(cuuint32_t)(ts.tw + 2 * GL), (cuuint32_t)(ts.th + 2 * HALF), (cuuint32_t)NV};
+  // dimensions (padded column, field, padded row); a box lands as [row][field][column]
+  cuuint64_t dims[3] = {(cuuint64_t)(L.n2 + 2 * GL), (cuuint64_t)NV, (cuuint64_t)(L.n1 + 2 * GT)};
+  cuuint64_t strides[2] = {(cuuint64_t)(L.FS * elem), (cuuint64_t)(L.RS * elem)};
+  cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)NV, (cuuint32_t)box_h};
   cuuint32_t estr[3] = {1, 1, 1};
   return encode(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
+}  // namespace
 
-template <class T, int TW, int TH, int NT, bool RV, bool WV, bool WU, bool CF>
-static cudaError_t run_substage(const CUtensorMap &tm, T *u_out, T *v, const Layout &L, const KParams<T> &kp,
-                                cudaStream_t s)
+CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
 {
-  using Cfg = SubstageCfg<T, TW, TH, NT>;
-  auto kern = substage_kernel<T, TW, TH, NT, RV, WV, WU, CF>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+  return encode_map(map, base, L, storage, sub::BW, sub::CH);
+}
+
+CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
+{
+  return encode_map(map, base, L, storage, sub::SW, sub::CH);
+}
+
+int substage_tiles(const Layout &L) { return sub::tile_grid(L).ntiles; }
+
+template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF>
+static cudaError_t run_substage(const CUtensorMap &mu, const CUtensorMap &mv, T *u_out, T *v, const Layout &L,
+                                const KParams<T> &kp, int *queue, cudaStream_t s)
+{
+  using G = sub::Geo<T>;
+  auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF>;
+  static int ctas_per_sm = 0, sms = 0;
+  if (!ctas_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
     if (e != cudaSuccess) return e;
-    configured = true;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, sub::NT, G::SMEM)) != cudaSuccess)
+      return e;
+    if (ctas_per_sm < 1) return cudaErrorInvalidConfiguration;
   }
-  const dim3 grid((L.n2 + TW - 1) / TW, (L.n1 + TH - 1) / TH);
-  kern<<<grid, NT, Cfg::SMEM, s>>>(tm, u_out, v, L, kp);
+  const int ntiles = sub::tile_grid(L).ntiles;
+  int grid = sms * ctas_per_sm;
+  if (grid > ntiles) grid = ntiles;
+  kern<<<grid, sub::NT, G::SMEM, s>>>(mu, mv, u_out, v, L, kp, queue);
   return cudaGetLastError();
 }
 
-template <class T, int TW, int TH, int NT>
-static cudaError_t substage_t(int kind, bool cfl, const CUtensorMap &tm, void *u_out, void *v, const Layout &L,
-                              const StageArgs &a, cudaStream_t s)
+template <class T, unsigned M2>
+static cudaError_t substage_m(int kind, bool cfl, const CUtensorMap &mu, const CUtensorMap &mv, T *uo, T *vv,
+                              const Layout &L, const KParams<T> &kp, int *queue, cudaStream_t s)
 {
-  const KParams<T> kp = make_params<T>(a);
-  T *uo = (T *)u_out, *vv = (T *)v;
   switch (kind) {
-    case STAGE_FIRST: return run_substage<T, TW, TH, NT, false, true, true, false>(tm, uo, vv, L, kp, s);
-    case STAGE_MID: return run_substage<T, TW, TH, NT, true, true, true, false>(tm, uo, vv, L, kp, s);
+    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false>(mu, mv, uo, vv, L, kp, queue, s);
+    case STAGE_MID: return run_substage<T, M2, true, true, true, false>(mu, mv, uo, vv, L, kp, queue, s);
     case STAGE_LAST:
-      return cfl ? run_substage<T, TW, TH, NT, true, false, true, true>(tm, uo, vv, L, kp, s)
-                 : run_substage<T, TW, TH, NT, true, false, true, false>(tm, uo, vv, L, kp, s);
-    case STAGE_KICK: return run_substage<T, TW, TH, NT, true, true, false, false>(tm, uo, vv, L, kp, s);
+      return cfl ? run_substage<T, M2, true, false, true, true>(mu, mv, uo, vv, L, kp, queue, s)
+                 : run_substage<T, M2, true, false, true, false>(mu, mv, uo, vv, L, kp, queue, s);
+    case STAGE_KICK: return run_substage<T, M2, true, true, false, false>(mu, mv, uo, vv, L, kp, queue, s);
   }
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_in_map, void *u_out, void *v,
-                            const Layout &L, const StageArgs &a, cudaStream_t s)
+// The kernels are compiled for two sets of second-derivative fields: the scheme's default
+// parameters' set, and all fields (correct for any parameters: an unused D11/D22 meets a
+// zero coefficient).  FP64, the reference-precision path, always uses all fields.
+template <class T>
+static cudaError_t substage_t(int kind, bool cfl, const CUtensorMap &mu, const CUtensorMap &mv, void *u_out, void *v,
+                              const Layout &L, const StageArgs &a, int *queue, cudaStream_t s)
 {
-  if (storage == ST_F32) return substage_t<float, TW32, TH32, NT32>(kind, cfl, u_in_map, u_out, v, L, a, s);
-  if (storage == ST_F64) return substage_t<double, TW64, TH64, NT64>(kind, cfl, u_in_map, u_out, v, L, a, s);
+  const KParams<T> kp = make_params<T>(a);
+  T *uo = (T *)u_out, *vv = (T *)v;
+  const unsigned need = scheme::d2_fields(a.para);
+  if constexpr (sizeof(T) == 4) {
+    if ((need & ~scheme::D2_DEFAULT) == 0)
+      return substage_m<T, scheme::D2_DEFAULT>(kind, cfl, mu, mv, uo, vv, L, kp, queue, s);
+  }
+  return substage_m<T, scheme::D2_ALL>(kind, cfl, mu, mv, uo, vv, L, kp, queue, s);
+}
+
+cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_map, const CUtensorMap &v_map,
+                            void *u_out, void *v, const Layout &L, const StageArgs &a, int *queue, cudaStream_t s)
+{
+  if (storage == ST_F32) return substage_t<float>(kind, cfl, u_map, v_map, u_out, v, L, a, queue, s);
+  if (storage == ST_F64) return substage_t<double>(kind, cfl, u_map, v_map, u_out, v, L, a, queue, s);
   return cudaErrorInvalidValue;
 }
 
@@ -546,11 +490,11 @@ cudaError_t launch_euler(int storage, void *u, const Layout &L, double dt, const
   const scheme::EulerArgs e{r1, r2};
   if (storage == ST_F32) {
     Para<float> p;
-    for (int q = 0; q < 8; ++q) p.v[q] = (float)para[q];
+    for (int q = 0; q < NPARA; ++q) p.v[q] = (float)para[q];
     euler_kernel<float><<<g, 256, 0, s>>>((float *)u, L, (float)dt, p, e, (float)delta1, (float)delta2);
   } else if (storage == ST_F64) {
     Para<double> p;
-    for (int q = 0; q < 8; ++q) p.v[q] = para[q];
+    for (int q = 0; q < NPARA; ++q) p.v[q] = para[q];
     euler_kernel<double><<<g, 256, 0, s>>>((double *)u, L, dt, p, e, delta1, delta2);
   } else
     return cudaErrorInvalidValue;
@@ -597,7 +541,7 @@ cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const
 {
   const int g = grid_for((long long)L.n1 * L.n2, 256);
   Para<double> p;
-  for (int q = 0; q < 8; ++q) p.v[q] = para[q];
+  for (int q = 0; q < NPARA; ++q) p.v[q] = para[q];
   if (storage == ST_F32)
     signal_max_kernel<float><<<g, 256, 0, s>>>((const float *)u, L, p, 1.0 / delta1, 1.0 / delta2, st);
   else if (storage == ST_F64)

@@ -33,19 +33,17 @@ enum StageKind : int {
   STAGE_KICK = 3,   // the reference's kick(): v <- F(u) + beta v only, u untouched
 };
 
-// Tile geometry of the fused substage kernel for a storage type.
-struct TileShape {
-  int tw, th, threads;
-  size_t smem;
-};
-TileShape substage_tile(int storage);
+// Tensor maps over one state array (all fields) in the device layout: u with the halo box
+// of one row chunk of the fused substage kernel, v with its interior box.  Return
+// CUDA_SUCCESS or the driver's error.
+CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
+CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
+int substage_tiles(const Layout &L);
 
-// Tensor map over one state array (all fields) in the device layout, with the box of
-// the substage kernel.  Returns CUDA_SUCCESS or the driver's error.
-CUresult encode_state_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
-
-cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_in_map, void *u_out, void *v,
-                            const Layout &L, const StageArgs &a, cudaStream_t s);
+// One fused substage over a whole grid.  `queue` is the simulation's tile queue: two ints,
+// zero before the first launch; every launch leaves them zero again.
+cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_map, const CUtensorMap &v_map,
+                            void *u_out, void *v, const Layout &L, const StageArgs &a, int *queue, cudaStream_t s);
 
 cudaError_t launch_bcond(int storage, void *u, const Layout &L, int p1, int p2, cudaStream_t s);
 cudaError_t launch_drift(int storage, void *u, const void *v, const Layout &L, double dt, Status *status,

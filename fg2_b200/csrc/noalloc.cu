@@ -121,7 +121,8 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
   if (n1 > NOALLOC_MAX_ROWS)
     return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: n1 = %d rows exceeds the scratch limit of %d rows", n1,
                      NOALLOC_MAX_ROWS);
-  if (pitch < (long long)n2 + 2 * GL || plane < (long long)(n1 + 2 * GT) * pitch)
+  // pitch = row stride, plane = field stride (element (f, i, j) at f * plane + (i + 3) * pitch + j + 4)
+  if (plane < (long long)n2 + 2 * GL || pitch < (long long)scheme::NVAR * plane)
     return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: pitch/plane too small for %d x %d", n1, n2);
   if (storage != ST_F32 && storage != ST_F64)
     return set_error(FG2_ERR_UNSUPPORTED, "fg2_sums_noalloc: storage %d not supported", storage);
@@ -131,8 +132,8 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
   Layout L;
   L.n1 = n1;
   L.n2 = n2;
-  L.P = pitch;
-  L.PS = plane;
+  L.RS = pitch;
+  L.FS = plane;
   cudaStream_t s = (cudaStream_t)stream;
   if (storage == ST_F32) row_sums_kernel<float><<<n1, NA_THREADS, 0, s>>>((const float *)u, L, scratch);
   else row_sums_kernel<double><<<n1, NA_THREADS, 0, s>>>((const double *)u, L, scratch);

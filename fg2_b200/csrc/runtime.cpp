@@ -81,13 +81,15 @@ struct fg2_sim {
   void *u[2] = {nullptr, nullptr};
   void *v = nullptr;
   int cur = 0;  // u[cur] holds the state
-  CUtensorMap map[2];
+  CUtensorMap map[2];     // u[0], u[1] with the substage kernel's halo box
+  CUtensorMap vmap;       // v with the interior box
+  int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   Status *status = nullptr;       // device
   Status *status_host = nullptr;  // pinned mirror
   double *sums_partial = nullptr, *sums_out = nullptr;
-  double para[8];
+  double para[NPARA];  // runtime keys by slot, then the scheme's derived constants
   double l1 = 1.0, l2 = 1.0, c = 0.5;  // src/global.cpp:28
   int p1 = 1, p2 = 1;                  // src/global.cpp:29
   double delta1 = 0, delta2 = 0;
@@ -102,13 +104,13 @@ struct fg2_sim {
   double graph_dt[2] = {0, 0}, graph_tend[2] = {0, 0};
   char para_msg[256];
   // the reference-mirror kick/drift may name arbitrary arrays: tensor map cache
-  const void *kick_map_base = nullptr;
-  CUtensorMap kick_map;
+  const void *kick_map_base = nullptr, *kick_vmap_base = nullptr;
+  CUtensorMap kick_map, kick_vmap;
 };
 
 namespace {
 
-size_t array_elems(const fg2_sim *s) { return (size_t)scheme::NVAR * (size_t)s->L.PS; }
+size_t array_elems(const fg2_sim *s) { return (size_t)s->L.elems(); }
 
 // Delta = l / n in the state's precision (src/config.cpp:39: R Delta[] = {l1/n1, l2/n2}).
 void compute_deltas(fg2_sim *s)
@@ -175,7 +177,7 @@ int do_euler(fg2_sim *s, double dt)
 bool euler_active(const fg2_sim *s)
 {
   Para<double> p;
-  for (int q = 0; q < 8; ++q) p.v[q] = s->para[q];
+  for (int q = 0; q < NPARA; ++q) p.v[q] = s->para[q];
   return scheme::euler_active<double>(p);
 }
 
@@ -193,8 +195,8 @@ int enqueue_step(fg2_sim *s, double dt, const double *dt_dev, bool cfl)
   for (int k = 0; k < 3; ++k) {
     const StageArgs a = stage_args(s, k, dt, dt_dev);
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-    CK(launch_substage(s->storage, kind, cfl && k == 2, s->map[s->cur], s->u[1 - s->cur], s->v, s->L, a,
-                       s->stream));
+    CK(launch_substage(s->storage, kind, cfl && k == 2, s->map[s->cur], s->vmap, s->u[1 - s->cur], s->v, s->L, a,
+                       s->queue, s->stream));
     s->cur = 1 - s->cur;
   }
   s->ghosts_valid = true;
@@ -270,9 +272,10 @@ int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, c
                        double *out)
 {
   if (!name || !out || n1 < 1 || n2 < 1) return fail(FG2_ERR_ARG, "bad arguments");
-  double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double p[NPARA] = {};
   for (int q = 0; q < scheme::NSLOT; ++q)
     p[scheme::PARA_KEYS[q].slot] = para ? para[q] : scheme::PARA_KEYS[q].def;
+  scheme::derive(p);
   scheme::settings(l1, l2);
   SetupCtx ctx{n1, n2, l1, l2, p, seed};
   std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
@@ -298,9 +301,10 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   s->n1 = n1;
   s->n2 = n2;
   s->storage = storage;
-  s->L = make_layout(n1, n2, elem_size(storage));
-  for (int q = 0; q < 8; ++q) s->para[q] = 0.0;
+  s->L = make_layout(n1, n2, scheme::NVAR, elem_size(storage));
+  for (int q = 0; q < NPARA; ++q) s->para[q] = 0.0;
   for (int q = 0; q < scheme::NSLOT; ++q) s->para[scheme::PARA_KEYS[q].slot] = round_para(s.get(), scheme::PARA_KEYS[q].def);
+  scheme::derive(s->para);
   if (stream) {
     s->stream = (cudaStream_t)stream;
   } else {
@@ -325,18 +329,21 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (cudaMalloc(&s->sums_partial, sizeof(double) * 4 * sums_blocks(s->L)) != cudaSuccess ||
       cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess)
     return cleanup("reduction scratch allocation failed");
-  for (int b = 0; b < 2; ++b)
-    if (encode_state_map(&s->map[b], s->u[b], s->L, storage) != CUDA_SUCCESS) {
-      fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
-      fg2_sim_destroy(s.release());
-      return nullptr;
-    }
+  if (cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess) return cleanup("queue allocation failed");
+  if (encode_u_map(&s->map[0], s->u[0], s->L, storage) != CUDA_SUCCESS ||
+      encode_u_map(&s->map[1], s->u[1], s->L, storage) != CUDA_SUCCESS ||
+      encode_v_map(&s->vmap, s->v, s->L, storage) != CUDA_SUCCESS) {
+    fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
+    fg2_sim_destroy(s.release());
+    return nullptr;
+  }
   // every array starts at -max like the reference (src/setup.cpp:80-83)
   const double lowest = storage == ST_F64 ? -std::numeric_limits<double>::max() : -std::numeric_limits<float>::max();
   if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->u[1], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->v, array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       cudaMemsetAsync(s->status, 0, sizeof(Status), s->stream) != cudaSuccess ||
+      cudaMemsetAsync(s->queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess)
     return cleanup("initial fill failed");
   return s.release();
@@ -354,6 +361,7 @@ void fg2_sim_destroy(fg2_sim *s)
   cudaFreeHost(s->status_host);
   cudaFree(s->sums_partial);
   cudaFree(s->sums_out);
+  cudaFree(s->queue);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -400,6 +408,7 @@ const char *fg2_sim_para(fg2_sim *s, const char *in)
     if (key == scheme::PARA_KEYS[q].name) {
       const double val = round_para(s, std::atof(eq + 1));
       s->para[scheme::PARA_KEYS[q].slot] = val;
+      scheme::derive(s->para);
       snprintf(s->para_msg, sizeof(s->para_msg), "%s = %g", key.c_str(), val);
       drop_graph(s);
       return s->para_msg;
@@ -591,7 +600,8 @@ int fg2_sim_stage(fg2_sim *s, int k, double dt)
   }
   const StageArgs a = stage_args(s, k, dt, nullptr);
   const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-  CK(launch_substage(s->storage, kind, false, s->map[s->cur], s->u[1 - s->cur], s->v, s->L, a, s->stream));
+  CK(launch_substage(s->storage, kind, false, s->map[s->cur], s->vmap, s->u[1 - s->cur], s->v, s->L, a, s->queue,
+                     s->stream));
   s->cur = 1 - s->cur;
   s->smax_valid = false;
   return FG2_OK;
@@ -637,7 +647,8 @@ int fg2_sim_kick(fg2_sim *s, double t, double beta)
   ensure_config(s);
   StageArgs a = stage_args(s, 0, 0.0, nullptr);
   a.beta = beta;
-  CK(launch_substage(s->storage, STAGE_KICK, false, s->map[s->cur], nullptr, s->v, s->L, a, s->stream));
+  CK(launch_substage(s->storage, STAGE_KICK, false, s->map[s->cur], s->vmap, nullptr, s->v, s->L, a, s->queue,
+                     s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return FG2_OK;
 }
@@ -706,8 +717,8 @@ void *fg2_sim_stream(fg2_sim *s) { return s ? (void *)s->stream : nullptr; }
 int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane)
 {
   if (!s) return fail(FG2_ERR_ARG, "null handle");
-  if (pitch) *pitch = s->L.P;
-  if (plane) *plane = s->L.PS;
+  if (pitch) *pitch = s->L.RS;
+  if (plane) *plane = s->L.FS;
   return FG2_OK;
 }
 
@@ -823,18 +834,26 @@ void fg2_kick(float *v, const float *u, float t, float beta)
   if (!g_sim) return;
   ensure_config(g_sim);
   const int ui = array_index(u);
-  const CUtensorMap *m = nullptr;
-  if (ui == 0 || ui == 1) m = &g_sim->map[ui];
+  const CUtensorMap *mu = nullptr, *mv = nullptr;
+  if (ui == 0 || ui == 1) mu = &g_sim->map[ui];
   else {
     if (g_sim->kick_map_base != u) {
-      if (encode_state_map(&g_sim->kick_map, u, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
+      if (encode_u_map(&g_sim->kick_map, u, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
       g_sim->kick_map_base = u;
     }
-    m = &g_sim->kick_map;
+    mu = &g_sim->kick_map;
+  }
+  if (v == g_sim->v) mv = &g_sim->vmap;
+  else {
+    if (g_sim->kick_vmap_base != v) {
+      if (encode_v_map(&g_sim->kick_vmap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
+      g_sim->kick_vmap_base = v;
+    }
+    mv = &g_sim->kick_vmap;
   }
   StageArgs a = stage_args(g_sim, 0, 0.0, nullptr);
   a.beta = beta;
-  launch_substage(g_sim->storage, STAGE_KICK, false, *m, nullptr, v, g_sim->L, a, g_sim->stream);
+  launch_substage(g_sim->storage, STAGE_KICK, false, *mu, *mv, nullptr, v, g_sim->L, a, g_sim->queue, g_sim->stream);
   cudaStreamSynchronize(g_sim->stream);
 }
 

@@ -18,6 +18,13 @@ template <class C>
 FG2_HD bool euler_active(const fg2::Para<C> &p) { return p.v[FAMP] * p.v[FK] > C(0); }
 
 template <class C>
+FG2_HD C fcos(C x);
+template <>
+FG2_HD float fcos<float>(float x) { return cosf(x); }
+template <>
+FG2_HD double fcos<double>(double x) { return cos(x); }
+
+template <class C>
 FG2_HD C fsin(C x);
 template <>
 FG2_HD float fsin<float>(float x) { return sinf(x); }

@@ -1,9 +1,8 @@
 // schemes/hydro/eqns.cuh -- right-hand side of the ideal-gas equations in log-primitive
 // form, with shear/bulk viscosity, viscous heating, thermal conduction and optional
-// density diffusion.  Physics and runtime keys follow src/hydro/eqns.cuh:19-92; the
-// derivatives arrive precomputed in a Cell (the kernel evaluates only the ones listed
-// by d2_fields()), and the arithmetic is arranged for the GPU: reciprocals instead of
-// divisions, 1/e instead of (gamma-1)/temp.
+// density diffusion.  Physics and runtime keys follow src/hydro/eqns.cuh:19-92.  The
+// derivatives arrive precomputed in a Cell; C is a scalar or a pair of cells (two cells per
+// thread, packed FP32x2 arithmetic), so every product-sum is written as an explicit fmac.
 #pragma once
 
 #include <cmath>
@@ -12,89 +11,86 @@
 
 namespace scheme {
 
-// Parameter slots and the reference defaults (src/hydro/eqns.cuh:19-24).
-enum Slot { GAMMA = 0, NUS = 1, NUB = 2, KAPPA = 3, DD = 4, NSLOT = 5 };
+// Parameter slots: the runtime keys with the reference defaults (src/hydro/eqns.cuh:19-24),
+// then constants derived from them once per launch on the host.
+enum Slot { GAMMA = 0, NUS = 1, NUB = 2, KAPPA = 3, DD = 4, NSLOT = 5,
+            GM1 = 5, NUS2 = 6, MIXED = 7, ED = 8, CSG = 9 };
 constexpr fg2::ParaKey PARA_KEYS[NSLOT] = {
     {"gamma", GAMMA, 5.0 / 3.0}, {"nus", NUS, 2.0e-4}, {"nub", NUB, 0.0},
     {"kappa", KAPPA, 5.0e-4},    {"dd", DD, 0.0}};
 
-// Fields whose second derivatives (D11, D22) the kernel must evaluate for these
-// parameters; D12 is needed for u1 and u2 only.
-template <class C>
-FG2_HD unsigned d2_fields(const fg2::Para<C> &p)
+// gamma - 1, 2 nus, nus / 3 + nub, (gamma - 1) kappa, sqrt(gamma (gamma - 1))
+inline void derive(double *v)
+{
+  v[GM1] = v[GAMMA] - 1.0;
+  v[NUS2] = 2.0 * v[NUS];
+  v[MIXED] = v[NUS] / 3.0 + v[NUB];
+  v[ED] = (v[GAMMA] - 1.0) * v[KAPPA];
+  v[CSG] = std::sqrt(v[GAMMA] * (v[GAMMA] - 1.0));
+}
+
+// Fields whose D11 and D22 the equations use for these parameters (u1 and u2 always, lne
+// when kappa != 0, lnd when dd != 0), and the two masks the kernels are compiled for.
+constexpr unsigned D2_DEFAULT = (1u << U1) | (1u << U2) | (1u << LNE);
+constexpr unsigned D2_ALL = (1u << U1) | (1u << U2) | (1u << LNE) | (1u << LND);
+constexpr unsigned D12_FIELDS = (1u << U1) | (1u << U2);
+inline unsigned d2_fields(const double *v)
 {
   unsigned m = (1u << U1) | (1u << U2);
-  if (p.v[DD] != C(0)) m |= 1u << LND;
-  if (p.v[KAPPA] != C(0)) m |= 1u << LNE;
+  if (v[DD] != 0.0) m |= 1u << LND;
+  if (v[KAPPA] != 0.0) m |= 1u << LNE;
   return m;
 }
-constexpr unsigned D12_FIELDS = (1u << U1) | (1u << U2);
 
-template <class C>
-FG2_HD C fexp(C x);
-template <>
-FG2_HD float fexp<float>(float x) { return expf(x); }
-template <>
-FG2_HD double fexp<double>(double x) { return exp(x); }
-
-// dq/dt at one cell.  i, j are the global cell indices and delta1 the axis-1 spacing
-// (all unused by this scheme).
-template <class C>
+// dq/dt at one cell (or cell pair).  M2 is the set of fields whose D11/D22 the caller
+// evaluated; the others read as zero.  i, j, delta1 are unused by this scheme.
+template <unsigned M2, class C>
 FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1)
 {
+  using fg2::fmac;
+  using fg2::lit;
   (void)i; (void)j; (void)delta1;
   const C u1 = c.q[U1], u2 = c.q[U2];
-  const C gamma = p.v[GAMMA], nus = p.v[NUS], nub = p.v[NUB];
-  const C gm1 = gamma - C(1);
-  const C ee = fexp(c.q[LNE]);        // specific thermal energy
-  const C temp = gm1 * ee;            // p / rho
-  const C iee = C(1) / ee;            // (gamma-1) / temp
+  const C ee = fg2::vexp(c.q[LNE]);    // specific thermal energy e
+  const C iee = fg2::vexp(-c.q[LNE]);  // (gamma - 1) / temp = 1 / e
+  const C temp = p.v[GM1] * ee;        // p / rho
   const C div = c.d1[U1] + c.d2[U2];
-  const C third = C(1.0 / 3.0);
+  const C m1 = lit<C>(-1.0);
 
-  // advection
-  C rl = -(u1 * c.d1[LND] + u2 * c.d2[LND]);
-  C r1 = -(u1 * c.d1[U1] + u2 * c.d2[U1]);
-  C r2 = -(u1 * c.d1[U2] + u2 * c.d2[U2]);
-  C re = -(u1 * c.d1[LNE] + u2 * c.d2[LNE]);
+  // terms of the form -(...): advection, compression, pressure gradient
+  const C nl = fmac(u1, c.d1[LND], fmac(u2, c.d2[LND], div));
+  const C n1 = fmac(u1, c.d1[U1], fmac(u2, c.d2[U1], temp * (c.d1[LND] + c.d1[LNE])));
+  const C n2 = fmac(u1, c.d1[U2], fmac(u2, c.d2[U2], temp * (c.d2[LND] + c.d2[LNE])));
+  const C ne = fmac(u1, c.d1[LNE], fmac(u2, c.d2[LNE], div * p.v[GM1]));
 
-  // compression and pressure gradient
-  rl -= div;
-  r1 -= temp * (c.d1[LND] + c.d1[LNE]);
-  r2 -= temp * (c.d2[LND] + c.d2[LNE]);
-  re -= div * gm1;
+  // viscous stress and its divergence, viscous heating
+  const C s11 = fmac(div, lit<C>(-1.0 / 3.0), c.d1[U1]);
+  const C s12 = (c.d1[U2] + c.d2[U1]) * lit<C>(0.5);
+  const C s22 = fmac(div, lit<C>(-1.0 / 3.0), c.d2[U2]);
+  C p1 = p.v[NUS2] * fmac(s11, c.d1[LND], s12 * c.d2[LND]);
+  C p2 = p.v[NUS2] * fmac(s12, c.d1[LND], s22 * c.d2[LND]);
+  p1 = fmac(p.v[NUS], c.d11[U1] + c.d22[U1], fmac(p.v[MIXED], c.d11[U1] + c.d12[U2], p1));
+  p2 = fmac(p.v[NUS], c.d11[U2] + c.d22[U2], fmac(p.v[MIXED], c.d12[U1] + c.d22[U2], p2));
+  const C heat = fmac(p.v[NUS2], fmac(s11, s11, fmac(s12 + s12, s12, s22 * s22)), p.v[NUB] * div * div);
 
-  // viscous force from the density gradient, viscous heating
-  const C s11 = c.d1[U1] - div * third;
-  const C s12 = (c.d1[U2] + c.d2[U1]) * C(0.5);
-  const C s22 = c.d2[U2] - div * third;
-  const C nus2 = C(2) * nus;
-  r1 += nus2 * (s11 * c.d1[LND] + s12 * c.d2[LND]);
-  r2 += nus2 * (s12 * c.d1[LND] + s22 * c.d2[LND]);
-  re += iee * (nus2 * (s11 * s11 + C(2) * s12 * s12 + s22 * s22) + nub * div * div);
-
-  // viscous stress divergence
-  const C mixed = nus * third + nub;
-  r1 += nus * (c.d11[U1] + c.d22[U1]) + mixed * (c.d11[U1] + c.d12[U2]);
-  r2 += nus * (c.d11[U2] + c.d22[U2]) + mixed * (c.d12[U1] + c.d22[U2]);
-
-  // density diffusion and thermal conduction (Laplacian of the log plus |grad|^2)
-  const C ed = gm1 * p.v[KAPPA];
-  rl += p.v[DD] * (c.d11[LND] + c.d22[LND] + (c.d1[LND] * c.d1[LND] + c.d2[LND] * c.d2[LND]));
-  re += ed * (c.d11[LNE] + c.d22[LNE] + (c.d1[LNE] * c.d1[LNE] + c.d2[LNE] * c.d2[LNE]));
-
-  r[LND] = rl;
-  r[U1] = r1;
-  r[U2] = r2;
-  r[LNE] = re;
+  // conduction (and density diffusion): Laplacian of the log plus |grad|^2
+  C pe = iee * heat;
+  if (M2 & (1u << LNE))
+    pe = fmac(p.v[ED], c.d11[LNE] + c.d22[LNE] + fmac(c.d1[LNE], c.d1[LNE], c.d2[LNE] * c.d2[LNE]), pe);
+  r[U1] = fmac(n1, m1, p1);
+  r[U2] = fmac(n2, m1, p2);
+  r[LNE] = fmac(ne, m1, pe);
+  if (M2 & (1u << LND))
+    r[LND] = fmac(nl, m1, p.v[DD] * (c.d11[LND] + c.d22[LND] + fmac(c.d1[LND], c.d1[LND], c.d2[LND] * c.d2[LND])));
+  else
+    r[LND] = nl * m1;
 }
 
-// Adiabatic sound speed sqrt(gamma (gamma-1) e) for the CFL condition.
+// Adiabatic sound speed sqrt(gamma (gamma - 1) e) = CSG exp(lne / 2), for the CFL condition.
 template <class C>
 FG2_HD C sound_speed(const C q[NVAR], const fg2::Para<C> &p)
 {
-  const C gamma = p.v[GAMMA];
-  return sqrt(gamma * (gamma - C(1)) * fexp(q[LNE]));
+  return p.v[CSG] * fg2::vexp(q[LNE] * fg2::lit<C>(0.5));
 }
 
 // Largest diffusion coefficient in the equations, for the explicit diffusive limit:

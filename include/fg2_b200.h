@@ -125,7 +125,8 @@ int fg2_sim_seed_forcing(fg2_sim *s, uint64_t seed);
  * reduction order (bitwise reproducible). */
 int fg2_sim_sums(fg2_sim *s, double out[4]);
 /* Current device arrays and their layout: element (f, i, j) at
- * base[f * plane + (i + 3) * pitch + (j + 4)], elements of the storage type. */
+ * base[f * plane + (i + 3) * pitch + (j + 4)], elements of the storage type; pitch is the
+ * stride of a grid row (all NVAR field rows of it), plane the stride between fields. */
 void *fg2_sim_u(fg2_sim *s);
 void *fg2_sim_v(fg2_sim *s);
 int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane);

@@ -41,9 +41,8 @@ def test_sums_noalloc_rejects_grids_beyond_the_scratch(cuda):
     lib = fg2_b200.load_library("hydro")
     out = torch.zeros(4, dtype=torch.float64, device=cuda)
     with fg2_b200.Sim(16, 16) as s:
-        pitch, _ = s.layout()
+        pitch, plane = s.layout()
         # rejected on the host before anything is launched
-        too_many = lib.fg2_sums_noalloc(lib.fg2_sim_u(s.h), 20000, 16, pitch, (20000 + 6) * pitch, 0,
-                                        out.data_ptr(), s.stream)
+        too_many = lib.fg2_sums_noalloc(lib.fg2_sim_u(s.h), 20000, 16, pitch, plane, 0, out.data_ptr(), s.stream)
     assert too_many == -1
     assert b"exceeds the scratch limit" in lib.fg2_last_error()
