@@ -47,14 +47,17 @@ struct PairOf<double> {
   static __host__ __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
 };
 
-// Parameters of one substage launch, rounded to the storage precision T and broadcast to
-// both lanes of a pair (so packed instructions read them straight from the constant bank).
+// Parameters of one substage launch, rounded to the storage precision T: the stencil
+// weights both as scalars and broadcast to both lanes of a pair (so packed instructions read
+// them straight from the constant bank), the scheme's parameters as scalars.
 template <class T>
 struct KParams {
   using P = typename PairOf<T>::type;
-  Coef<P> k;
-  Para<P> p;
-  P beta;
+  Coef<P> k;   // packed stencil weights
+  Coef<T> ks;  // scalar stencil weights
+  Para<T> p;   // scheme parameters
+  P beta2;     // the stage's beta on both lanes
+  int store_cols;  // interior columns the bulk stores cover (the rest are stored per thread)
   double gamma, dt;
   const double *dt_dev;
   int p1, p2;
@@ -78,22 +81,37 @@ static KParams<T> make_params(const StageArgs &a)
   const double w2[4] = {-490. / 180., 270. / 180., -27. / 180., 2. / 180.};
   const double wm[3] = {270. / 720., -27. / 720., 2. / 720.};
   for (int q = 0; q < 3; ++q) {
-    kp.k.a1[q] = bc<T>(w1[q] / d1);
-    kp.k.a2[q] = bc<T>(w1[q] / d2);
-    kp.k.m[q] = bc<T>(wm[q] / (d1 * d2));
-    kp.k.mn[q] = bc<T>(-wm[q] / (d1 * d2));
+    kp.ks.a1[q] = (T)(w1[q] / d1);
+    kp.ks.a2[q] = (T)(w1[q] / d2);
+    kp.ks.m[q] = (T)(wm[q] / (d1 * d2));
+    kp.ks.mn[q] = (T)(-wm[q] / (d1 * d2));
   }
   for (int q = 0; q < 4; ++q) {
-    kp.k.b1[q] = bc<T>(w2[q] / (d1 * d1));
-    kp.k.b2[q] = bc<T>(w2[q] / (d2 * d2));
+    kp.ks.b1[q] = (T)(w2[q] / (d1 * d1));
+    kp.ks.b2[q] = (T)(w2[q] / (d2 * d2));
   }
-  kp.k.delta1 = bc<T>(d1);
-  kp.k.delta2 = bc<T>(d2);
-  kp.k.inv1 = bc<T>(1.0 / d1);
-  kp.k.inv2 = bc<T>(1.0 / d2);
-  for (int q = 0; q < NPARA; ++q) kp.p.v[q] = bc<T>(a.para ? a.para[q] : 0.0);
-  kp.beta = bc<T>(a.beta);
+  kp.ks.delta1 = (T)d1;
+  kp.ks.delta2 = (T)d2;
+  kp.ks.inv1 = (T)(1.0 / d1);
+  kp.ks.inv2 = (T)(1.0 / d2);
+  for (int q = 0; q < 3; ++q) {
+    kp.k.a1[q] = bc<T>(kp.ks.a1[q]);
+    kp.k.a2[q] = bc<T>(kp.ks.a2[q]);
+    kp.k.m[q] = bc<T>(kp.ks.m[q]);
+    kp.k.mn[q] = bc<T>(kp.ks.mn[q]);
+  }
+  for (int q = 0; q < 4; ++q) {
+    kp.k.b1[q] = bc<T>(kp.ks.b1[q]);
+    kp.k.b2[q] = bc<T>(kp.ks.b2[q]);
+  }
+  kp.k.delta1 = bc<T>(kp.ks.delta1);
+  kp.k.delta2 = bc<T>(kp.ks.delta2);
+  kp.k.inv1 = bc<T>(kp.ks.inv1);
+  kp.k.inv2 = bc<T>(kp.ks.inv2);
+  for (int q = 0; q < NPARA; ++q) kp.p.v[q] = (T)(a.para ? a.para[q] : 0.0);
+  kp.beta2 = bc<T>(a.beta);
   kp.gamma = a.gamma;
+  kp.store_cols = a.store_cols;
   kp.dt = a.dt;
   kp.dt_dev = a.dt_dev;
   kp.p1 = a.p1;
@@ -125,6 +143,24 @@ __device__ __forceinline__ Images ghost_images(int i, int j, int n1, int n2, int
   if (j < HALF) { g.cols[g.nc] = p2 ? j + n2 : -1 - j; g.flip[g.nc++] = !p2; }
   if (j >= n2 - HALF) { g.cols[g.nc] = p2 ? j - n2 : 2 * n2 - 1 - j; g.flip[g.nc++] = !p2; }
   return g;
+}
+
+// Only the ghost images of (i, j), not the cell itself (which the caller stores).
+template <class T, class C>
+__device__ __forceinline__ void store_ghosts(T *u, const Layout &L, int i, int j, const C q[NV], int p1, int p2)
+{
+  const bool edge = i < HALF || i >= L.n1 - HALF || j < HALF || j >= L.n2 - HALF;
+  if (!edge) return;
+  const Images g = ghost_images(i, j, L.n1, L.n2, p1, p2);
+  for (int a = 0; a < g.nr; ++a)
+    for (int b = 0; b < g.nc; ++b) {
+      if (a == 0 && b == 0) continue;
+#pragma unroll
+      for (int f = 0; f < NV; ++f) {
+        const C x = (g.flip[b] && scheme::reflect_sign(f) < 0) ? -q[f] : q[f];
+        u[L.at(f, g.rows[a], g.cols[b])] = (T)x;
+      }
+    }
 }
 
 template <class T, class C>
@@ -171,7 +207,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
   return encode;
 }
 
-CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int storage, int box_w, int box_h)
+// ext_w, ext_h: extents of the padded column and row dimensions the map covers
+CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int storage, int box_w, int box_h, long long ext_w,
+                    long long ext_h)
 {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (!encode) return CUDA_ERROR_NOT_FOUND;
@@ -181,7 +219,7 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
                                  : storage == ST_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                      : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   // dimensions (padded column, field, padded row); a box lands as [row][field][column]
-  cuuint64_t dims[3] = {(cuuint64_t)(L.n2 + 2 * GL), (cuuint64_t)NV, (cuuint64_t)(L.n1 + 2 * GT)};
+  cuuint64_t dims[3] = {(cuuint64_t)ext_w, (cuuint64_t)NV, (cuuint64_t)ext_h};
   cuuint64_t strides[2] = {(cuuint64_t)(L.FS * elem), (cuuint64_t)(L.RS * elem)};
   cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)NV, (cuuint32_t)box_h};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -192,19 +230,36 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
 
 CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
 {
-  return encode_map(map, base, L, storage, sub::BW, sub::CH);
+  return encode_map(map, base, L, storage, sub::BW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
 }
 
 CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
 {
-  return encode_map(map, base, L, storage, sub::SW, sub::CH);
+  return encode_map(map, base, L, storage, sub::SW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+}
+
+// Interior columns a bulk store may write: a bulk store clips a box at the map's extent only
+// to whole 16-byte chunks of the innermost dimension, so the store map ends at the last chunk
+// that lies entirely inside the interior; the (at most 3) interior columns after it are
+// stored by their threads.
+int store_cols(const Layout &L, int storage)
+{
+  const int vec = storage == ST_F64 ? 2 : storage == ST_F32 ? 4 : 8;
+  return (L.n2 + GL) / vec * vec - GL;
+}
+
+// Store map: ends at the last interior row (padded n1 + GT - 1) and at column store_cols - 1,
+// so a bulk store of a partial tile writes no ghost cell.
+CUresult encode_store_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
+{
+  return encode_map(map, base, L, storage, sub::SW, sub::CH, store_cols(L, storage) + GL, L.n1 + GT);
 }
 
 int substage_tiles(const Layout &L) { return sub::tile_grid(L).ntiles; }
 
 template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF>
-static cudaError_t run_substage(const CUtensorMap &mu, const CUtensorMap &mv, T *u_out, T *v, const Layout &L,
-                                const KParams<T> &kp, int *queue, cudaStream_t s)
+static cudaError_t run_substage(const StageMaps &m, T *u_out, T *v, const Layout &L, const KParams<T> &kp, int *queue,
+                                cudaStream_t s)
 {
   using G = sub::Geo<T>;
   auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF>;
@@ -222,21 +277,21 @@ static cudaError_t run_substage(const CUtensorMap &mu, const CUtensorMap &mv, T 
   const int ntiles = sub::tile_grid(L).ntiles;
   int grid = sms * ctas_per_sm;
   if (grid > ntiles) grid = ntiles;
-  kern<<<grid, sub::NT, G::SMEM, s>>>(mu, mv, u_out, v, L, kp, queue);
+  kern<<<grid, sub::NT, G::SMEM, s>>>(*m.u_in, *m.v_in, *m.u_out, *m.v_out, u_out, v, L, kp, queue);
   return cudaGetLastError();
 }
 
 template <class T, unsigned M2>
-static cudaError_t substage_m(int kind, bool cfl, const CUtensorMap &mu, const CUtensorMap &mv, T *uo, T *vv,
-                              const Layout &L, const KParams<T> &kp, int *queue, cudaStream_t s)
+static cudaError_t substage_m(int kind, bool cfl, const StageMaps &m, T *uo, T *vv, const Layout &L,
+                              const KParams<T> &kp, int *queue, cudaStream_t s)
 {
   switch (kind) {
-    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false>(mu, mv, uo, vv, L, kp, queue, s);
-    case STAGE_MID: return run_substage<T, M2, true, true, true, false>(mu, mv, uo, vv, L, kp, queue, s);
+    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false>(m, uo, vv, L, kp, queue, s);
+    case STAGE_MID: return run_substage<T, M2, true, true, true, false>(m, uo, vv, L, kp, queue, s);
     case STAGE_LAST:
-      return cfl ? run_substage<T, M2, true, false, true, true>(mu, mv, uo, vv, L, kp, queue, s)
-                 : run_substage<T, M2, true, false, true, false>(mu, mv, uo, vv, L, kp, queue, s);
-    case STAGE_KICK: return run_substage<T, M2, true, true, false, false>(mu, mv, uo, vv, L, kp, queue, s);
+      return cfl ? run_substage<T, M2, true, false, true, true>(m, uo, vv, L, kp, queue, s)
+                 : run_substage<T, M2, true, false, true, false>(m, uo, vv, L, kp, queue, s);
+    case STAGE_KICK: return run_substage<T, M2, true, true, false, false>(m, uo, vv, L, kp, queue, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -245,24 +300,24 @@ static cudaError_t substage_m(int kind, bool cfl, const CUtensorMap &mu, const C
 // parameters' set, and all fields (correct for any parameters: an unused D11/D22 meets a
 // zero coefficient).  FP64, the reference-precision path, always uses all fields.
 template <class T>
-static cudaError_t substage_t(int kind, bool cfl, const CUtensorMap &mu, const CUtensorMap &mv, void *u_out, void *v,
-                              const Layout &L, const StageArgs &a, int *queue, cudaStream_t s)
+static cudaError_t substage_t(int kind, bool cfl, const StageMaps &m, void *u_out, void *v, const Layout &L,
+                              const StageArgs &a, int *queue, cudaStream_t s)
 {
   const KParams<T> kp = make_params<T>(a);
   T *uo = (T *)u_out, *vv = (T *)v;
   const unsigned need = scheme::d2_fields(a.para);
   if constexpr (sizeof(T) == 4) {
     if ((need & ~scheme::D2_DEFAULT) == 0)
-      return substage_m<T, scheme::D2_DEFAULT>(kind, cfl, mu, mv, uo, vv, L, kp, queue, s);
+      return substage_m<T, scheme::D2_DEFAULT>(kind, cfl, m, uo, vv, L, kp, queue, s);
   }
-  return substage_m<T, scheme::D2_ALL>(kind, cfl, mu, mv, uo, vv, L, kp, queue, s);
+  return substage_m<T, scheme::D2_ALL>(kind, cfl, m, uo, vv, L, kp, queue, s);
 }
 
-cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_map, const CUtensorMap &v_map,
-                            void *u_out, void *v, const Layout &L, const StageArgs &a, int *queue, cudaStream_t s)
+cudaError_t launch_substage(int storage, int kind, bool cfl, const StageMaps &m, void *u_out, void *v, const Layout &L,
+                            const StageArgs &a, int *queue, cudaStream_t s)
 {
-  if (storage == ST_F32) return substage_t<float>(kind, cfl, u_map, v_map, u_out, v, L, a, queue, s);
-  if (storage == ST_F64) return substage_t<double>(kind, cfl, u_map, v_map, u_out, v, L, a, queue, s);
+  if (storage == ST_F32) return substage_t<float>(kind, cfl, m, u_out, v, L, a, queue, s);
+  if (storage == ST_F64) return substage_t<double>(kind, cfl, m, u_out, v, L, a, queue, s);
   return cudaErrorInvalidValue;
 }
 

@@ -24,6 +24,7 @@ struct StageArgs {
   const double *para;   // scheme parameters by slot
   int p1, p2;           // boundary kind per axis (BC_PERIODIC / BC_WALL)
   Status *status;       // device status block
+  int store_cols;       // interior columns covered by the bulk-store maps (store_cols())
 };
 
 enum StageKind : int {
@@ -34,16 +35,24 @@ enum StageKind : int {
 };
 
 // Tensor maps over one state array (all fields) in the device layout: u with the halo box
-// of one row chunk of the fused substage kernel, v with its interior box.  Return
+// of one row chunk of the fused substage kernel, v with its interior box, and the store map
+// (interior box, extents ending at the interior) that bulk stores write through.  Return
 // CUDA_SUCCESS or the driver's error.
 CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
 CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
+CUresult encode_store_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
+int store_cols(const Layout &L, int storage);
 int substage_tiles(const Layout &L);
+
+// The four maps one substage launch uses: u read (halo box), v prefetched, u' stored, v stored.
+struct StageMaps {
+  const CUtensorMap *u_in, *v_in, *u_out, *v_out;
+};
 
 // One fused substage over a whole grid.  `queue` is the simulation's tile queue: two ints,
 // zero before the first launch; every launch leaves them zero again.
-cudaError_t launch_substage(int storage, int kind, bool cfl, const CUtensorMap &u_map, const CUtensorMap &v_map,
-                            void *u_out, void *v, const Layout &L, const StageArgs &a, int *queue, cudaStream_t s);
+cudaError_t launch_substage(int storage, int kind, bool cfl, const StageMaps &maps, void *u_out, void *v,
+                            const Layout &L, const StageArgs &a, int *queue, cudaStream_t s);
 
 cudaError_t launch_bcond(int storage, void *u, const Layout &L, int p1, int p2, cudaStream_t s);
 cudaError_t launch_drift(int storage, void *u, const void *v, const Layout &L, double dt, Status *status,

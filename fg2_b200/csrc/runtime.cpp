@@ -83,6 +83,8 @@ struct fg2_sim {
   int cur = 0;  // u[cur] holds the state
   CUtensorMap map[2];     // u[0], u[1] with the substage kernel's halo box
   CUtensorMap vmap;       // v with the interior box
+  CUtensorMap omap[2];    // u[0], u[1] store maps (interior)
+  CUtensorMap vomap;      // v store map (interior)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -105,7 +107,7 @@ struct fg2_sim {
   char para_msg[256];
   // the reference-mirror kick/drift may name arbitrary arrays: tensor map cache
   const void *kick_map_base = nullptr, *kick_vmap_base = nullptr;
-  CUtensorMap kick_map, kick_vmap;
+  CUtensorMap kick_map, kick_vmap, kick_vomap;
 };
 
 namespace {
@@ -140,6 +142,7 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p1 = s->p1;
   a.p2 = s->p2;
   a.status = s->status;
+  a.store_cols = store_cols(s->L, s->storage);
   return a;
 }
 
@@ -195,8 +198,8 @@ int enqueue_step(fg2_sim *s, double dt, const double *dt_dev, bool cfl)
   for (int k = 0; k < 3; ++k) {
     const StageArgs a = stage_args(s, k, dt, dt_dev);
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-    CK(launch_substage(s->storage, kind, cfl && k == 2, s->map[s->cur], s->vmap, s->u[1 - s->cur], s->v, s->L, a,
-                       s->queue, s->stream));
+    const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
+    CK(launch_substage(s->storage, kind, cfl && k == 2, m, s->u[1 - s->cur], s->v, s->L, a, s->queue, s->stream));
     s->cur = 1 - s->cur;
   }
   s->ghosts_valid = true;
@@ -332,7 +335,10 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess) return cleanup("queue allocation failed");
   if (encode_u_map(&s->map[0], s->u[0], s->L, storage) != CUDA_SUCCESS ||
       encode_u_map(&s->map[1], s->u[1], s->L, storage) != CUDA_SUCCESS ||
-      encode_v_map(&s->vmap, s->v, s->L, storage) != CUDA_SUCCESS) {
+      encode_v_map(&s->vmap, s->v, s->L, storage) != CUDA_SUCCESS ||
+      encode_store_map(&s->omap[0], s->u[0], s->L, storage) != CUDA_SUCCESS ||
+      encode_store_map(&s->omap[1], s->u[1], s->L, storage) != CUDA_SUCCESS ||
+      encode_store_map(&s->vomap, s->v, s->L, storage) != CUDA_SUCCESS) {
     fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
     fg2_sim_destroy(s.release());
     return nullptr;
@@ -600,8 +606,8 @@ int fg2_sim_stage(fg2_sim *s, int k, double dt)
   }
   const StageArgs a = stage_args(s, k, dt, nullptr);
   const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-  CK(launch_substage(s->storage, kind, false, s->map[s->cur], s->vmap, s->u[1 - s->cur], s->v, s->L, a, s->queue,
-                     s->stream));
+  const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
+  CK(launch_substage(s->storage, kind, false, m, s->u[1 - s->cur], s->v, s->L, a, s->queue, s->stream));
   s->cur = 1 - s->cur;
   s->smax_valid = false;
   return FG2_OK;
@@ -647,8 +653,8 @@ int fg2_sim_kick(fg2_sim *s, double t, double beta)
   ensure_config(s);
   StageArgs a = stage_args(s, 0, 0.0, nullptr);
   a.beta = beta;
-  CK(launch_substage(s->storage, STAGE_KICK, false, s->map[s->cur], s->vmap, nullptr, s->v, s->L, a, s->queue,
-                     s->stream));
+  const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
+  CK(launch_substage(s->storage, STAGE_KICK, false, m, nullptr, s->v, s->L, a, s->queue, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return FG2_OK;
 }
@@ -843,17 +849,24 @@ void fg2_kick(float *v, const float *u, float t, float beta)
     }
     mu = &g_sim->kick_map;
   }
-  if (v == g_sim->v) mv = &g_sim->vmap;
-  else {
+  const CUtensorMap *mvo = nullptr;
+  if (v == g_sim->v) {
+    mv = &g_sim->vmap;
+    mvo = &g_sim->vomap;
+  } else {
     if (g_sim->kick_vmap_base != v) {
-      if (encode_v_map(&g_sim->kick_vmap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
+      if (encode_v_map(&g_sim->kick_vmap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS ||
+          encode_store_map(&g_sim->kick_vomap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS)
+        return;
       g_sim->kick_vmap_base = v;
     }
     mv = &g_sim->kick_vmap;
+    mvo = &g_sim->kick_vomap;
   }
   StageArgs a = stage_args(g_sim, 0, 0.0, nullptr);
   a.beta = beta;
-  launch_substage(g_sim->storage, STAGE_KICK, false, *mu, *mv, nullptr, v, g_sim->L, a, g_sim->queue, g_sim->stream);
+  const StageMaps m{mu, mv, mvo, mvo};
+  launch_substage(g_sim->storage, STAGE_KICK, false, m, nullptr, v, g_sim->L, a, g_sim->queue, g_sim->stream);
   cudaStreamSynchronize(g_sim->stream);
 }
 

@@ -4,28 +4,30 @@
 // Work decomposition.  A tile is a strip of SW = 128 interior columns by TH = 35 rows of one
 // simulation.  A persistent grid of CTAs drains a tile queue (an atomic counter that the
 // last CTA to finish resets, so a launch needs no host-side reset and replays from a CUDA
-// graph).  Each CTA has NCW = 2 warps; a thread owns the two columns t and t + 64 of the
-// strip and evaluates both cells with one stream of pair instructions (packed FP32x2 on
-// sm_100: add/mul/fma .f32x2).
+// graph).  A CTA has 4 warps; a thread owns one column of the strip.
 //
 // Data movement.  u streams through a ring of NSLOT shared-memory slots by TMA
 // (cp.async.bulk.tensor.3d, no multicast): chunk 0 of a tile is the 7-row warm-up box
 // u[i0-4 .. i0+3) x [j0-4, j0+132) (all fields), chunk b+1 the 7 leading rows u[i0+3+7b ..]
-// of output block b; a box lands as [row][field][column].  v never enters shared memory:
-// when a block's u chunk is issued, the same 7 rows of v are prefetched into L2
-// (cp.async.bulk.prefetch.tensor), and each thread reads its v values with coalesced loads
-// issued at the top of the row that updates them.  There is no producer warp: the warp that
-// releases a slot last refills it.  Full mbarriers carry the TMA completion, empty
-// mbarriers the releases; every wait is bounded (%globaltimer) and a timeout raises an
-// error bit in the status block.
+// of output block b; a box lands as [row][field][column].  When a block's u chunk is
+// issued, the same 7 rows of v are prefetched into L2 (cp.async.bulk.prefetch.tensor), and
+// each thread loads its v values a row before it needs them.  The block's results (u' and
+// the new v) are staged in shared memory and written back with one TMA tensor store per
+// array; the store maps end at the interior's last row and column, so partial tiles clip
+// there and ghost cells are never written by the bulk store (edge cells write their ghost
+// images directly).  One CTA barrier per chunk hands the ring slot and the staging buffer
+// over; every wait on a TMA completion is bounded (%globaltimer) and the CTA agrees on a
+// timeout before leaving, which raises an error bit in the status block.
 //
-// Stencil.  Each thread walks its columns down the tile.  At every leading row L it loads
-// the 7 values u(L, j-3..j+3) of each field from shared memory and computes the axis-2
+// Stencil.  Each thread walks its column down the tile.  At every leading row L it loads the
+// 7 values u(L, j-3..j+3) of each field from shared memory and computes the axis-2
 // (contiguous) derivatives D2 and D22 of row L, pushes u(L, j) into a 7-row register window
 // (the axis-1 stencil of row L-3 then needs no further loads), and feeds the mixed
 // derivative by streaming accumulators: with delta_k(r) = u(r, j+k) - u(r, j-k),
 // D12(r) = sum_k m_k (delta_k(r+k) - delta_k(r-k)), so delta_k(L) is added to row L-k and
-// subtracted from row L+k (src/deriv.h:60-62 regrouped).  The output row L-3 then has all its
+// subtracted from row L+k (src/deriv.h:60-62 regrouped).  Fields are handled in pairs
+// ((lnd, u1), (u2, lne)) so the stencil arithmetic of two fields is one packed FP32x2
+// instruction (add/mul/fma .f32x2 on sm_100).  The output row L-3 then has all its
 // derivatives in registers; the scheme's eqns() gives F, and the epilogue applies
 // v <- F + beta v, u' <- u + gamma dt v (src/kick.cu:53, src/drift.cu:29), stores u' with
 // its ghost images and v, flags NaNs and, on the last stage, folds the CFL rate into a max.
@@ -36,17 +38,21 @@
 namespace sub {
 
 constexpr int SW = 128;            // interior columns per tile (strip width)
-constexpr int HW = SW / 2;         // distance between the two columns of a thread
 constexpr int BW = SW + 2 * GL;    // TMA box width of u (halo 4 + 4; the stencil uses 3)
 constexpr int CH = 7;              // rows per chunk = register window period
 constexpr int NB = 5;              // output blocks per tile
 constexpr int TH = NB * CH;        // output rows per tile
-constexpr int NCW = 2;             // warps per CTA
-constexpr int NT = NCW * 32;       // threads per CTA
-static_assert(NT == HW, "one thread per column pair");
+constexpr int NCW = 4;             // warps per CTA
+constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
+constexpr int NP = (NV + 1) / 2;   // field pairs
+static_assert(NT == SW, "one thread per strip column");
+static_assert(scheme::U1 == 1 && scheme::U2 == 2, "u1 and u2 are fields 1 and 2");
 
 #ifndef FG2_NSLOT_F32
 #define FG2_NSLOT_F32 2
+#endif
+#ifndef FG2_MIN_CTAS
+#define FG2_MIN_CTAS 1
 #endif
 
 template <class T>
@@ -54,10 +60,12 @@ struct Geo {
   static constexpr int NSLOT = sizeof(T) == 8 ? 2 : FG2_NSLOT_F32;
   static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * NV * sizeof(T));
   static constexpr uint32_t SLOT = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
-  static constexpr size_t BAR_OFF = (size_t)NSLOT * SLOT;
-  // tail: full[NSLOT], empty[NSLOT] (mbarriers), rel[NSLOT], tile_of[NSLOT], producer state
-  static constexpr size_t SMEM = BAR_OFF + 2 * NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 4 * sizeof(int) + 64;
-  static_assert(SLOT % 128 == 0, "TMA shared-memory destinations must be 128-byte aligned");
+  static constexpr uint32_t OUT_BYTES = (uint32_t)(SW * CH * NV * sizeof(T));  // one block of one array
+  static constexpr size_t STAGE_OFF = (size_t)NSLOT * SLOT;                     // u' then v staging
+  static constexpr size_t BAR_OFF = STAGE_OFF + 2 * (size_t)OUT_BYTES;
+  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], producer state
+  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + NSLOT * sizeof(int) + 4 * sizeof(int) + 64;
+  static_assert(SLOT % 128 == 0 && OUT_BYTES % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
   static_assert(BW <= 256 && CH <= 256, "TMA box dimensions");
   static_assert((BW * sizeof(T)) % 16 == 0 && (SW * sizeof(T)) % 16 == 0, "TMA rows must be 16-byte multiples");
 };
@@ -77,13 +85,21 @@ __host__ __device__ inline TileGrid tile_grid(const Layout &L)
   return g;
 }
 
+// Does field f carry second derivatives (D11, D22) under mask M2?
+template <unsigned M2>
+__host__ __device__ constexpr bool need(int f)
+{
+  return f < NV && (M2 & (1u << f));
+}
+
 // Per-thread rolling state.  Slot index = leading-row index mod 7.
-template <class C>
+template <class T>
 struct Roll {
-  C w[NV][CH];     // u(row, j), rows L-6 .. L
-  C h2[NV][CH];    // D2 of each row
-  C h22[NV][CH];   // D22 of each row
-  C x[2][CH];      // D12 accumulators of u1, u2
+  using P = typename PairOf<T>::type;
+  P w[NP][CH];    // u(row, j) per field pair, rows L-6 .. L
+  P h2[NP][CH];   // D2 of each row
+  P h22[NP][CH];  // D22 of each row (only the lanes under the mask are written)
+  T x[2][CH];     // D12 accumulators of u1, u2
 };
 
 __device__ __forceinline__ bool bounded_wait(uint64_t *bar, uint32_t parity, Status *st)
@@ -98,118 +114,169 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Leading-row work for register slot R: loads row R of the chunk for both columns.
-template <class T, unsigned M2, int R>
-__device__ __forceinline__ void lead_row(const T *su, int tx, const Coef<typename PairOf<T>::type> &k,
-                                         Roll<typename PairOf<T>::type> &s)
+// Leading-row work of field pair PI for register slot R.
+template <class T, unsigned M2, int R, int PI>
+__device__ __forceinline__ void lead_pair(const T *row, const KParams<T> &a, Roll<T> &s,
+                                          typename PairOf<T>::type dk[3])
 {
-  using C = typename PairOf<T>::type;
+  using P = typename PairOf<T>::type;
   using PO = PairOf<T>;
-  const T *p0 = su + R * (NV * BW) + tx + GL;
-#pragma unroll
-  for (int f = 0; f < NV; ++f) {
-    const T *p = p0 + f * BW;
-    const C c = PO::make(p[0], p[HW]);
-    const C l1 = PO::make(p[-1], p[HW - 1]), r1 = PO::make(p[1], p[HW + 1]);
-    const C l2 = PO::make(p[-2], p[HW - 2]), r2 = PO::make(p[2], p[HW + 2]);
-    const C l3 = PO::make(p[-3], p[HW - 3]), r3 = PO::make(p[3], p[HW + 3]);
-    s.w[f][R] = c;
-    const C d1 = r1 - l1, d2 = r2 - l2, d3 = r3 - l3;
-    s.h2[f][R] = fmac(k.a2[0], d1, fmac(k.a2[1], d2, k.a2[2] * d3));
-    if (M2 & (1u << f))
-      s.h22[f][R] = fmac(k.b2[0], c, fmac(k.b2[1], r1 + l1, fmac(k.b2[2], r2 + l2, k.b2[3] * (r3 + l3))));
-    if (scheme::D12_FIELDS & (1u << f)) {
-      const int g = f == scheme::U1 ? 0 : 1;
-      // rows L+k get -m_k delta_k(L) (mn = -m), rows L-k get +m_k delta_k(L); row L-3 is
-      // then complete.  The first contribution to row L+3 initialises its accumulator.
-      s.x[g][(R + 3) % CH] = k.mn[2] * d3;
-      s.x[g][(R + 2) % CH] = fmac(k.mn[1], d2, s.x[g][(R + 2) % CH]);
-      s.x[g][(R + 1) % CH] = fmac(k.mn[0], d1, s.x[g][(R + 1) % CH]);
-      s.x[g][(R + 6) % CH] = fmac(k.m[0], d1, s.x[g][(R + 6) % CH]);
-      s.x[g][(R + 5) % CH] = fmac(k.m[1], d2, s.x[g][(R + 5) % CH]);
-      s.x[g][(R + 4) % CH] = fmac(k.m[2], d3, s.x[g][(R + 4) % CH]);
-    }
+  constexpr bool two = 2 * PI + 1 < NV;
+  const T *q0 = row + (2 * PI) * BW;
+  const T *q1 = q0 + BW;
+  const P c = PO::make(q0[0], two ? q1[0] : T(0));
+  const P l1 = PO::make(q0[-1], two ? q1[-1] : T(0)), r1 = PO::make(q0[1], two ? q1[1] : T(0));
+  const P l2 = PO::make(q0[-2], two ? q1[-2] : T(0)), r2 = PO::make(q0[2], two ? q1[2] : T(0));
+  const P l3 = PO::make(q0[-3], two ? q1[-3] : T(0)), r3 = PO::make(q0[3], two ? q1[3] : T(0));
+  s.w[PI][R] = c;
+  dk[0] = r1 - l1;
+  dk[1] = r2 - l2;
+  dk[2] = r3 - l3;
+  s.h2[PI][R] = fmac(a.k.a2[0], dk[0], fmac(a.k.a2[1], dk[1], a.k.a2[2] * dk[2]));
+  constexpr bool nx = need<M2>(2 * PI), ny = need<M2>(2 * PI + 1);
+  if constexpr (nx && ny) {
+    s.h22[PI][R] = fmac(a.k.b2[0], c, fmac(a.k.b2[1], r1 + l1, fmac(a.k.b2[2], r2 + l2, a.k.b2[3] * (r3 + l3))));
+  } else if constexpr (nx) {
+    s.h22[PI][R].x = fmac(a.ks.b2[0], c.x, fmac(a.ks.b2[1], r1.x + l1.x,
+                                                fmac(a.ks.b2[2], r2.x + l2.x, a.ks.b2[3] * (r3.x + l3.x))));
+  } else if constexpr (ny) {
+    s.h22[PI][R].y = fmac(a.ks.b2[0], c.y, fmac(a.ks.b2[1], r1.y + l1.y,
+                                                fmac(a.ks.b2[2], r2.y + l2.y, a.ks.b2[3] * (r3.y + l3.y))));
   }
 }
 
-// v values of output row i for both columns (coalesced loads, issued a row ahead of use).
+// Leading-row work for register slot R: loads row R of the chunk.
+template <class T, unsigned M2, int R>
+__device__ __forceinline__ void lead_row(const T *su, int tx, const KParams<T> &a, Roll<T> &s)
+{
+  using P = typename PairOf<T>::type;
+  const T *row = su + R * (NV * BW) + tx + GL;
+  P dk[NP][3];
+  lead_pair<T, M2, R, 0>(row, a, s, dk[0]);
+  if constexpr (NP > 1) lead_pair<T, M2, R, 1>(row, a, s, dk[1]);
+  // D12 of u1 (pair 0, lane y) and u2 (pair 1, lane x): rows L+k get -m_k delta_k(L) (mn = -m),
+  // rows L-k get +m_k delta_k(L); row L-3 is then complete.  The first contribution to row
+  // L+3 initialises its accumulator.
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    const T d1 = g == 0 ? dk[0][0].y : dk[1][0].x;
+    const T d2 = g == 0 ? dk[0][1].y : dk[1][1].x;
+    const T d3 = g == 0 ? dk[0][2].y : dk[1][2].x;
+    s.x[g][(R + 3) % CH] = a.ks.mn[2] * d3;
+    s.x[g][(R + 2) % CH] = fmac(a.ks.mn[1], d2, s.x[g][(R + 2) % CH]);
+    s.x[g][(R + 1) % CH] = fmac(a.ks.mn[0], d1, s.x[g][(R + 1) % CH]);
+    s.x[g][(R + 6) % CH] = fmac(a.ks.m[0], d1, s.x[g][(R + 6) % CH]);
+    s.x[g][(R + 5) % CH] = fmac(a.ks.m[1], d2, s.x[g][(R + 5) % CH]);
+    s.x[g][(R + 4) % CH] = fmac(a.ks.m[2], d3, s.x[g][(R + 4) % CH]);
+  }
+}
+
+// v of output row i (pairs of fields), loaded a row before use; `ok` false skips the load.
 template <class T, bool READ_V>
-__device__ __forceinline__ void load_v(const T *v, const Layout &L, int i, int j,
-                                       typename PairOf<T>::type vr[NV])
+__device__ __forceinline__ void load_v(const T *v, const Layout &L, int i, int j, bool ok,
+                                       typename PairOf<T>::type vr[NP])
 {
   if (!READ_V) return;
-  const bool row_ok = i < L.n1, okx = row_ok && j < L.n2, oky = row_ok && j + HW < L.n2;
-  const T *p = v + L.at(0, i, j);
+  ok = ok && i < L.n1 && j < L.n2;
+  const T *q = v + L.at(0, i, j);
 #pragma unroll
-  for (int f = 0; f < NV; ++f) {
-    vr[f].x = okx ? __ldcs(p + f * L.FS) : T(0);
-    vr[f].y = oky ? __ldcs(p + f * L.FS + HW) : T(0);
+  for (int p = 0; p < NP; ++p) {
+    vr[p].x = ok ? __ldcs(q + (2 * p) * L.FS) : T(0);
+    vr[p].y = (ok && 2 * p + 1 < NV) ? __ldcs(q + (2 * p + 1) * L.FS) : T(0);
+  }
+}
+
+// Derivatives of field pair PI at the output row held in register slot S0, into a Cell.
+template <class T, unsigned M2, int S0, int PI>
+__device__ __forceinline__ void emit_pair(const KParams<T> &a, const Roll<T> &s, Cell<T, NV> &cell)
+{
+  using P = typename PairOf<T>::type;
+  const P c = s.w[PI][S0];
+  const P p1 = s.w[PI][(S0 + 1) % CH], n1 = s.w[PI][(S0 + 6) % CH];
+  const P p2 = s.w[PI][(S0 + 2) % CH], n2 = s.w[PI][(S0 + 5) % CH];
+  const P p3 = s.w[PI][(S0 + 3) % CH], n3 = s.w[PI][(S0 + 4) % CH];
+  const P d1 = fmac(a.k.a1[0], p1 - n1, fmac(a.k.a1[1], p2 - n2, a.k.a1[2] * (p3 - n3)));
+  const P d2 = s.h2[PI][S0];
+  constexpr bool nx = need<M2>(2 * PI), ny = need<M2>(2 * PI + 1);
+  P d11 = lit<P>(0.0), d22 = lit<P>(0.0);
+  if constexpr (nx && ny) {
+    d11 = fmac(a.k.b1[0], c, fmac(a.k.b1[1], p1 + n1, fmac(a.k.b1[2], p2 + n2, a.k.b1[3] * (p3 + n3))));
+    d22 = s.h22[PI][S0];
+  } else if constexpr (nx) {
+    d11.x = fmac(a.ks.b1[0], c.x, fmac(a.ks.b1[1], p1.x + n1.x, fmac(a.ks.b1[2], p2.x + n2.x, a.ks.b1[3] * (p3.x + n3.x))));
+    d22.x = s.h22[PI][S0].x;
+  } else if constexpr (ny) {
+    d11.y = fmac(a.ks.b1[0], c.y, fmac(a.ks.b1[1], p1.y + n1.y, fmac(a.ks.b1[2], p2.y + n2.y, a.ks.b1[3] * (p3.y + n3.y))));
+    d22.y = s.h22[PI][S0].y;
+  }
+  cell.q[2 * PI] = c.x;
+  cell.d1[2 * PI] = d1.x;
+  cell.d2[2 * PI] = d2.x;
+  cell.d11[2 * PI] = d11.x;
+  cell.d22[2 * PI] = d22.x;
+  if constexpr (2 * PI + 1 < NV) {
+    cell.q[2 * PI + 1] = c.y;
+    cell.d1[2 * PI + 1] = d1.y;
+    cell.d2[2 * PI + 1] = d2.y;
+    cell.d11[2 * PI + 1] = d11.y;
+    cell.d22[2 * PI + 1] = d22.y;
   }
 }
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
+// Results go to the block's staging buffers (rows [R][field][column]); edge cells also write
+// their ghost images to u_out.
 template <class T, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
-__device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NV], int i, int j, const KParams<T> &a,
-                                         const Layout &L, typename PairOf<T>::type gdt, T *u_out, T *v,
-                                         const Roll<typename PairOf<T>::type> &s, bool &nan, T &rate)
+__device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], int i, int j, int tx,
+                                         const KParams<T> &a, typename PairOf<T>::type gdt2, const Layout &L,
+                                         T *stage_u, T *stage_v, T *u_out, T *v, const Roll<T> &s, bool &nan, T &rate)
 {
-  using C = typename PairOf<T>::type;
+  using P = typename PairOf<T>::type;
   constexpr int S0 = (R + 4) % CH;
-  const C zero = lit<C>(0.0);
-  Cell<C, NV> cell;
+  Cell<T, NV> cell;
+  emit_pair<T, M2, S0, 0>(a, s, cell);
+  if constexpr (NP > 1) emit_pair<T, M2, S0, 1>(a, s, cell);
 #pragma unroll
-  for (int f = 0; f < NV; ++f) {
-    const C c = s.w[f][S0];
-    const C p1 = s.w[f][(S0 + 1) % CH], n1 = s.w[f][(S0 + 6) % CH];
-    const C p2 = s.w[f][(S0 + 2) % CH], n2 = s.w[f][(S0 + 5) % CH];
-    const C p3 = s.w[f][(S0 + 3) % CH], n3 = s.w[f][(S0 + 4) % CH];
-    cell.q[f] = c;
-    cell.d1[f] = fmac(a.k.a1[0], p1 - n1, fmac(a.k.a1[1], p2 - n2, a.k.a1[2] * (p3 - n3)));
-    if (M2 & (1u << f)) {
-      cell.d11[f] = fmac(a.k.b1[0], c, fmac(a.k.b1[1], p1 + n1, fmac(a.k.b1[2], p2 + n2, a.k.b1[3] * (p3 + n3))));
-      cell.d22[f] = s.h22[f][S0];
-    } else {
-      cell.d11[f] = zero;
-      cell.d22[f] = zero;
-    }
-    cell.d2[f] = s.h2[f][S0];
-    cell.d12[f] = (scheme::D12_FIELDS & (1u << f)) ? s.x[f == scheme::U1 ? 0 : 1][S0] : zero;
-  }
-  if (i >= L.n1) return;
-  C r[NV];
-  scheme::eqns<M2>(cell, a.p, i, j, r, a.k.delta1);
-  const bool okx = j < L.n2, oky = j + HW < L.n2;
-  const long long o = L.at(0, i, j);
-  C qn[NV];
+  for (int f = 0; f < NV; ++f) cell.d12[f] = T(0);
+  cell.d12[scheme::U1] = s.x[0][S0];
+  cell.d12[scheme::U2] = s.x[1][S0];
+
+  T r[NV];
+  scheme::eqns<M2>(cell, a.p, i, j, r, a.ks.delta1);
+  T qn[NV];
 #pragma unroll
-  for (int f = 0; f < NV; ++f) {
-    C vn = r[f];
-    if (READ_V) vn = fmac(a.beta, vr[f], vn);
+  for (int p = 0; p < NP; ++p) {
+    const bool two = 2 * p + 1 < NV;
+    P vn = PairOf<T>::make(r[2 * p], two ? r[2 * p + 1] : T(0));
+    if (READ_V) vn = fmac(a.beta2, vr[p], vn);
+    const P qp = fmac(gdt2, vn, PairOf<T>::make(cell.q[2 * p], two ? cell.q[2 * p + 1] : T(0)));
     if (WRITE_V) {
-      if (okx) v[o + f * L.FS] = vn.x;
-      if (oky) v[o + f * L.FS + HW] = vn.y;
+      stage_v[(R * NV + 2 * p) * SW + tx] = vn.x;
+      if (two) stage_v[(R * NV + 2 * p + 1) * SW + tx] = vn.y;
     }
-    qn[f] = fmac(gdt, vn, cell.q[f]);
-    nan |= (okx && qn[f].x != qn[f].x) || (oky && qn[f].y != qn[f].y);
+    qn[2 * p] = qp.x;
+    if (two) qn[2 * p + 1] = qp.y;
   }
   if (WRITE_U) {
-    T qx[NV], qy[NV];
+#pragma unroll
+    for (int f = 0; f < NV; ++f) stage_u[(R * NV + f) * SW + tx] = qn[f];
+  }
+  if (i >= L.n1 || j >= L.n2) return;  // cells past the grid: staged values are clipped by the store
+#pragma unroll
+  for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
+  if (j >= a.store_cols) {  // interior columns past the bulk stores' last whole 16-byte chunk
+    const long long o = L.at(0, i, j);
 #pragma unroll
     for (int f = 0; f < NV; ++f) {
-      qx[f] = qn[f].x;
-      qy[f] = qn[f].y;
+      if (WRITE_U) u_out[o + f * L.FS] = qn[f];
+      if (WRITE_V) v[o + f * L.FS] = stage_v[(R * NV + f) * SW + tx];
     }
-    if (okx) store_images<T, T>(u_out, L, i, j, qx, a.p1, a.p2);
-    if (oky) store_images<T, T>(u_out, L, i, j + HW, qy, a.p1, a.p2);
   }
-  if (CFL) {
-    const C cr = cfl_rate<C>(qn, a.p, a.k);
-    if (okx) rate = fmax(rate, cr.x);
-    if (oky) rate = fmax(rate, cr.y);
-  }
+  if (WRITE_U) store_ghosts<T, T>(u_out, L, i, j, qn, a.p1, a.p2);
+  if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, a.ks));
 }
 
-// Shared state of the refill duty, handed from warp to warp through shared memory.
+// Shared state of the chunk issue, read and written by thread 0 only.
 struct Producer {
   int next_n;  // index of the next chunk to issue
   int tile;    // tile of that chunk
@@ -248,36 +315,32 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
   ps->next_n = n + 1;
 }
 
-#ifndef FG2_MIN_CTAS
-#define FG2_MIN_CTAS 1
-#endif
-
 template <class T, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
 __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid_constant__ CUtensorMap tm_u,
-                                                      const __grid_constant__ CUtensorMap tm_v,
-                                                      T *__restrict__ u_out, T *__restrict__ v, const Layout L,
-                                                      const KParams<T> a, int *queue)
+                                                                    const __grid_constant__ CUtensorMap tm_v,
+                                                                    const __grid_constant__ CUtensorMap tm_uo,
+                                                                    const __grid_constant__ CUtensorMap tm_vo,
+                                                                    T *__restrict__ u_out, T *__restrict__ v,
+                                                                    const Layout L, const KParams<T> a, int *queue)
 {
-  using C = typename PairOf<T>::type;
+  using P = typename PairOf<T>::type;
   using G = Geo<T>;
   constexpr int NS = G::NSLOT;
   extern __shared__ __align__(128) unsigned char smem[];
+  T *stage_u = reinterpret_cast<T *>(smem + G::STAGE_OFF);
+  T *stage_v = reinterpret_cast<T *>(smem + G::STAGE_OFF + G::OUT_BYTES);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
-  uint64_t *empty = full + NS;
-  int *rel = reinterpret_cast<int *>(empty + NS);
-  int *tile_of = rel + NS;
+  int *tile_of = reinterpret_cast<int *>(full + NS);
   Producer *ps = reinterpret_cast<Producer *>(tile_of + NS);
-  const int lane = threadIdx.x & 31;
   const TileGrid tg = tile_grid(L);
+  const int lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
     prefetch_tmap(&tm_u);
     if (READ_V) prefetch_tmap(&tm_v);
-    for (int s = 0; s < NS; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NCW);
-      rel[s] = 0;
-    }
+    if (WRITE_U) prefetch_tmap(&tm_uo);
+    if (WRITE_V) prefetch_tmap(&tm_vo);
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
     ps->next_n = 0;
     ps->tile = -1;
@@ -289,64 +352,70 @@ __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid
 
   bool nan = false;
   T rate = T(0);
-  const int tx = threadIdx.x;  // first column within the strip; the second is tx + 64
-  const C gdt = lit<C>(a.gamma * (a.dt_dev ? *a.dt_dev : a.dt));  // (R)(dt * gamma[i]), src/step.cpp:34
-  Roll<C> st;
-  int n = 0;       // chunks consumed
-  bool ok = true;
+  const int tx = threadIdx.x;  // column within the strip
+  const P gdt2 = lit<P>(a.gamma * (a.dt_dev ? *a.dt_dev : a.dt));  // (R)(dt * gamma[i]), src/step.cpp:34
+  Roll<T> st;
+  int n = 0;  // chunks consumed
+  int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
+  P vr[2][NP];
 
-  // Release slot s of chunk n; the warp that releases last refills it.
-  auto release = [&](int s) {
-    __syncwarp();
-    if (lane == 0) {
-      mbar_arrive(&empty[s]);
-      if (atomicAdd(&rel[s], 1) == NCW - 1) {
-        rel[s] = 0;
-        if (mbar_wait_bounded(&empty[s], (uint32_t)((n / NS) & 1), WAIT_NS))
-          issue_chunk<T, READ_V>(ps, smem, full, tile_of, &tm_u, &tm_v, queue, tg);
-        else
-          atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-      }
+  for (;;) {
+    const int s = n % NS;
+    // the chunk has landed (every thread waits, the CTA agrees) and, for thread 0's last
+    // bulk stores, the staging buffers have been read out
+    if (threadIdx.x == 0 && (WRITE_U || WRITE_V)) bulk_wait_read_all();
+    const bool landed = mbar_wait_bounded(&full[s], (uint32_t)((n / NS) & 1), WAIT_NS);
+    if (__syncthreads_or(!landed)) {
+      if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
+      break;
     }
-  };
-
-  while (ok) {
-    int s = n % NS;
-    if (!bounded_wait(&full[s], (uint32_t)((n / NS) & 1), a.status)) break;
-    const int tile = tile_of[s];
-    if (tile < 0) break;
-    const int i0 = (tile / tg.strips) * TH;
-    const int j = (tile % tg.strips) * SW + tx;
+    const T *su = reinterpret_cast<const T *>(smem + (size_t)s * G::SLOT);
+    if (b < 0) {
+      const int tile = tile_of[s];
+      if (tile < 0) break;
+      i0 = (tile / tg.strips) * TH;
+      j0 = (tile % tg.strips) * SW;
 #pragma unroll
-    for (int g = 0; g < 2; ++g)
+      for (int g = 0; g < 2; ++g)
 #pragma unroll
-      for (int q = 0; q < CH; ++q) st.x[g][q] = lit<C>(0.0);
-    {  // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
-      const T *su = reinterpret_cast<const T *>(smem + (size_t)s * G::SLOT);
-      lead_row<T, M2, 0>(su, tx, a.k, st);
-      lead_row<T, M2, 1>(su, tx, a.k, st);
-      lead_row<T, M2, 2>(su, tx, a.k, st);
-      lead_row<T, M2, 3>(su, tx, a.k, st);
-      lead_row<T, M2, 4>(su, tx, a.k, st);
-      lead_row<T, M2, 5>(su, tx, a.k, st);
-      lead_row<T, M2, 6>(su, tx, a.k, st);
-    }
-    release(s);
-    ++n;
-    for (int b = 0; b < NB; ++b, ++n) {
-      s = n % NS;
-      if (!bounded_wait(&full[s], (uint32_t)((n / NS) & 1), a.status)) { ok = false; break; }
-      const T *su = reinterpret_cast<const T *>(smem + (size_t)s * G::SLOT);
-      const int ib = i0 + CH * b;
-      C vr[NV];
+        for (int q = 0; q < CH; ++q) st.x[g][q] = T(0);
+      load_v<T, READ_V>(v, L, i0, j0 + tx, true, vr[0]);  // v of the tile's first output row
+      // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
+      lead_row<T, M2, 0>(su, tx, a, st);
+      lead_row<T, M2, 1>(su, tx, a, st);
+      lead_row<T, M2, 2>(su, tx, a, st);
+      lead_row<T, M2, 3>(su, tx, a, st);
+      lead_row<T, M2, 4>(su, tx, a, st);
+      lead_row<T, M2, 5>(su, tx, a, st);
+      lead_row<T, M2, 6>(su, tx, a, st);
+    } else {
+      const int ib = i0 + CH * b, j = j0 + tx;
+      // row R uses vr[R & 1] and loads the next row into vr[(R + 1) & 1]; a block has an odd
+      // number of rows, so it ends by moving the loaded row to vr[0]
 #define FG2_ROW(R)                                                                                        \
-  load_v<T, READ_V>(v, L, ib + R, j, vr);                                                                 \
-  lead_row<T, M2, R>(su, tx, a.k, st);                                                                    \
-  emit_row<T, M2, R, READ_V, WRITE_V, WRITE_U, CFL>(vr, ib + R, j, a, L, gdt, u_out, v, st, nan, rate);
+  load_v<T, READ_V>(v, L, ib + R + 1, j, CH * b + R + 1 < TH, vr[(R + 1) & 1]);                           \
+  lead_row<T, M2, R>(su, tx, a, st);                                                                      \
+  emit_row<T, M2, R, READ_V, WRITE_V, WRITE_U, CFL>(vr[R & 1], ib + R, j, tx, a, gdt2, L, stage_u, stage_v, \
+                                                    u_out, v, st, nan, rate);
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
-      release(s);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) vr[0][p] = vr[1][p];
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // staged results -> bulk stores
     }
+    __syncthreads();  // everyone is done with slot s and has staged its results
+    if (threadIdx.x == 0) {
+      if (b >= 0 && i0 + CH * b < L.n1) {
+        // interior rows ib .. ib+6 of the strip; the maps clip at the last interior row/column
+        const int ib = i0 + CH * b;
+        if (WRITE_U) tma_store_3d(&tm_uo, stage_u, j0 + GL, 0, ib + GT);
+        if (WRITE_V) tma_store_3d(&tm_vo, stage_v, j0 + GL, 0, ib + GT);
+        if (WRITE_U || WRITE_V) bulk_commit();
+      }
+      issue_chunk<T, READ_V>(ps, smem, full, tile_of, &tm_u, &tm_v, queue, tg);  // refill slot s
+    }
+    ++n;
+    b = b == NB - 1 ? -1 : b + 1;
   }
 
   if (WRITE_U) {
@@ -361,7 +430,8 @@ __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid
 
   __syncthreads();
   if (threadIdx.x == 0) {
-    // after an error, let every copy this CTA issued land before the CTA exits
+    if (WRITE_U || WRITE_V) bulk_wait_all();  // the bulk stores have completed
+    // after an error, let every load this CTA issued land before the CTA exits
     const int issued = ps->next_n;
     for (int s = 0; s < NS && s < issued; ++s) {
       const int last = s + ((issued - 1 - s) / NS) * NS;  // last chunk issued into slot s
