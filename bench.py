@@ -163,10 +163,14 @@ def cpu_sample(state, rows, steps, dt):
     return rows * N2 * steps / el / 1e9, kind, cores, el
 
 
-def calibrated_rows(state, dt, budget_s, per_steps):
-    rate, _, _, _ = cpu_sample(state, 32, 1, dt)
-    rows = int(budget_s * rate * 1e9 / (N2 * per_steps))
-    return max(16, min(N1, rows))
+def calibrated_sample(state, dt, budget_s, min_steps=1):
+    """(rows, steps) of a CPU sample that takes about `budget_s` seconds: a strip of the
+    state for short budgets, the whole grid and more steps for long ones."""
+    rate, _, _, _ = cpu_sample(state, 256, 1, dt)
+    cells = budget_s * rate * 1e9
+    steps = max(min_steps, int(cells // (N1 * N2)))
+    rows = int(cells / (N2 * steps))
+    return max(16, min(N1, rows)), steps
 
 
 def initial_state():
@@ -181,21 +185,21 @@ def run_reference(args):
         return
     state = initial_state()
     dt = CPU_DT
-    rows = calibrated_rows(state, dt, 120.0 / max(1, args.steps + args.warmup), 1)
+    rows, per = calibrated_sample(state, dt, 120.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
-        cpu_sample(state, rows, 1, dt)
+        cpu_sample(state, rows, per, dt)
     el = 0.0
     for _ in range(args.steps):
-        _, kind, cores, e = cpu_sample(state, rows, 1, dt)
+        _, kind, cores, e = cpu_sample(state, rows, per, dt)
         el += e
-    value = rows * N2 * args.steps / el / 1e9
+    value = rows * N2 * per * args.steps / el / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3 * (N1 / rows),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / (args.steps * per) * 1e3 * (N1 / rows),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "scheme": SCHEME, "grid": [N1, N2]},
         "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
-                         "sample": f"each step: one RK3 step on a periodic {rows}x{N2} strip of the 4096^2 state"},
+                         "sample": f"each step: {per} RK3 step(s) on a periodic {rows}x{N2} strip of the 4096^2 state"},
         "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ns_per_cell_step": 1.0 / value,
     }
@@ -295,10 +299,10 @@ def run_fused(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rows = calibrated_rows(state, CPU_DT, 15.0, 2)
-        rate, kind, cores, el = cpu_sample(state, rows, 2, CPU_DT)
+        rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
+        rate, kind, cores, el = cpu_sample(state, rows, per, CPU_DT)
         cpu = {"value": rate, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
-               "sample": f"2 RK3 steps on a periodic {rows}x{N2} strip of the 4096^2 state ({el:.1f} s)"}
+               "sample": f"{per} RK3 steps on a periodic {rows}x{N2} strip of the 4096^2 state ({el:.1f} s)"}
 
     if rank == 0:
         line = {
