@@ -65,7 +65,7 @@ def _bind(lib):
         "fg2_kick": (None, [P, P, ctypes.c_float, ctypes.c_float]),
         "fg2_drift": (None, [P, P, ctypes.c_float]), "fg2_bcond": (None, [P, I, I]),
         "fg2_Euler": (None, [P, ctypes.c_float]), "fg2_global": (P, []),
-        "fg2_sums_noalloc": (I, [P, I, I, LL, LL, I, P, P]),
+        "fg2_sums_noalloc": (I, [P, I, I, LL, I, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1,15 +1,17 @@
 // fg2_b200/csrc/fg2b.h -- shared host/device definitions of the B200 time-step library.
 //
-// Device layout of one simulation (rows of field segments): element (f, i, j),
+// Device layout of one simulation: cells of NVAR interleaved fields (the reference's own
+// cell layout, src/setup.cpp:60-72) in rows with ghost rows and columns.  Element (f, i, j),
 // i in [-3, n1+3), j in [-4, n2+4), lives at
-//       base[f * FS + (i + GT) * RS + (j + GL)]
+//       base[(i + GT) * RS + (j + GL) * CS + f]            CS = NVAR
 //   GT = 3 ghost rows above/below (HALF of the 6th-order stencil, src/fg2.h:26-34);
 //   GL = 4 columns left of the interior: 3 ghosts plus one so that the interior and every
 //   tile's halo start on a 16-byte boundary (a TMA box must start on one);
-//   FS = field stride = P >= n2 + 8, rounded up so every field row starts on 128 bytes;
-//   RS = row stride = NVAR * P (the NVAR field rows of grid row i are consecutive).
-// Axis 1 (i, n1, Delta1) is the slow, strided axis and axis 2 (j, n2, Delta2) the
-// contiguous one, as in the reference (src/deriv.h:33, src/init.cpp:31-35).
+//   RS = row stride = PC * NVAR, PC >= n2 + 8 cells rounded up to a multiple of 32, so every
+//   row starts on 128 bytes and holds whole 16-byte groups of cells.
+// A 128-cell tile row of one array is one contiguous 2 KB (FP32 hydro) segment.  Axis 1
+// (i, n1, Delta1) is the slow, strided axis and axis 2 (j, n2, Delta2) the contiguous one,
+// as in the reference (src/deriv.h:33, src/init.cpp:31-35).
 #pragma once
 
 #include <cmath>
@@ -42,19 +44,18 @@ enum Bc : int { BC_WALL = 0, BC_PERIODIC = 1 };
 struct Layout {
   int n1, n2;
   long long RS;  // row stride, elements
-  long long FS;  // field stride, elements
-  FG2_HD long long at(int f, int i, int j) const { return f * FS + (long long)(i + GT) * RS + (j + GL); }
+  int CS;        // cell stride, elements (NVAR)
+  FG2_HD long long at(int f, int i, int j) const { return (long long)(i + GT) * RS + (long long)(j + GL) * CS + f; }
   FG2_HD long long elems() const { return (long long)(n1 + 2 * GT) * RS; }
 };
 
-inline Layout make_layout(int n1, int n2, int nvar, size_t elem)
+inline Layout make_layout(int n1, int n2, int nvar)
 {
   Layout L;
   L.n1 = n1;
   L.n2 = n2;
-  const long long align = 128 / (long long)elem;
-  L.FS = ((long long)n2 + 2 * GL + align - 1) / align * align;
-  L.RS = nvar * L.FS;
+  L.CS = nvar;
+  L.RS = ((long long)n2 + 2 * GL + 31) / 32 * 32 * nvar;
   return L;
 }
 

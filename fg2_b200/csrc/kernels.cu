@@ -207,21 +207,28 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
   return encode;
 }
 
-// ext_w, ext_h: extents of the padded column and row dimensions the map covers
-CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int storage, int box_w, int box_h, long long ext_w,
-                    long long ext_h)
+// Cells per 16-byte group: TMA boxes are built from whole groups, so the innermost box
+// dimension (one group of interleaved cells, NV x 16 bytes) is a 16-byte multiple for any
+// NVAR and the innermost coordinate is always 0.
+int group_cells(int storage) { return storage == ST_F64 ? 2 : storage == ST_F32 ? 4 : 8; }
+
+// Map over the padded array as (group element, cell group, padded row): box_cells x box_rows
+// boxes land in shared memory as [row][cell][field]; the map covers ext_cells cells (whole
+// groups) and ext_rows rows.
+CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int storage, int box_cells, int box_rows,
+                    long long ext_cells, long long ext_rows)
 {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (!encode) return CUDA_ERROR_NOT_FOUND;
   const size_t elem = storage == ST_F64 ? 8 : (storage == ST_F32 ? 4 : 2);
+  const int G = group_cells(storage);
   const CUtensorMapDataType dt = storage == ST_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                  : storage == ST_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : storage == ST_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                      : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  // dimensions (padded column, field, padded row); a box lands as [row][field][column]
-  cuuint64_t dims[3] = {(cuuint64_t)ext_w, (cuuint64_t)NV, (cuuint64_t)ext_h};
-  cuuint64_t strides[2] = {(cuuint64_t)(L.FS * elem), (cuuint64_t)(L.RS * elem)};
-  cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)NV, (cuuint32_t)box_h};
+  cuuint64_t dims[3] = {(cuuint64_t)(G * NV), (cuuint64_t)((ext_cells + G - 1) / G), (cuuint64_t)ext_rows};
+  cuuint64_t strides[2] = {(cuuint64_t)(G * NV * elem), (cuuint64_t)(L.RS * elem)};
+  cuuint32_t box[3] = {(cuuint32_t)(G * NV), (cuuint32_t)(box_cells / G), (cuuint32_t)box_rows};
   cuuint32_t estr[3] = {1, 1, 1};
   return encode(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -238,14 +245,14 @@ CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int s
   return encode_map(map, base, L, storage, sub::SW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
 }
 
-// Interior columns a bulk store may write: a bulk store clips a box at the map's extent only
-// to whole 16-byte chunks of the innermost dimension, so the store map ends at the last chunk
-// that lies entirely inside the interior; the (at most 3) interior columns after it are
-// stored by their threads.
+// Interior columns a bulk store may write: a store clips a box at the map's extent only at
+// whole cell groups, so the store map ends at the last group that lies entirely inside the
+// interior; the (fewer than one group of) interior columns after it are stored by their
+// threads.
 int store_cols(const Layout &L, int storage)
 {
-  const int vec = storage == ST_F64 ? 2 : storage == ST_F32 ? 4 : 8;
-  return (L.n2 + GL) / vec * vec - GL;
+  const int G = group_cells(storage);
+  return (L.n2 + GL) / G * G - GL;
 }
 
 // Store map: ends at the last interior row (padded n1 + GT - 1) and at column store_cols - 1,
@@ -359,17 +366,15 @@ __global__ void bcond_kernel(T *u, const Layout L, int p1, int p2)
   }
 }
 
-// drift (src/drift.cu:23-32): u <- u + dt v over the interior, NaN flag.
+// drift (src/drift.cu:23-32): u <- u + dt v over the interior, NaN flag.  Interior rows
+// are contiguous runs of n2 * NVAR elements.
 template <class T>
 __global__ void drift_kernel(T *u, const T *v, const Layout L, T dt, Status *st)
 {
-  const long long n = (long long)NV * L.n1 * L.n2;
+  const long long run = (long long)L.n2 * NV, n = run * L.n1;
   bool nan = false;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    const int f = (int)(k / ((long long)L.n1 * L.n2));
-    const long long rem = k % ((long long)L.n1 * L.n2);
-    const int i = (int)(rem / L.n2), j = (int)(rem % L.n2);
-    const long long o = L.at(f, i, j);
+    const long long o = L.at(0, (int)(k / run), 0) + k % run;
     const T x = fma(dt, v[o], u[o]);
     u[o] = x;
     nan |= x != x;
@@ -397,31 +402,6 @@ template <class T>
 __global__ void fill_kernel(T *p, size_t n, T x)
 {
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) p[k] = x;
-}
-
-// host layout (rows i0 .. i0 + nrows, cells of NV interleaved values) -> device layout
-template <class T, class H>
-__global__ void scatter_kernel(T *u, const H *src, const Layout L, int i0, int nrows)
-{
-  const long long n = (long long)nrows * L.n2 * NV;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    const int f = (int)(k % NV);
-    const long long cell = k / NV;
-    const int i = i0 + (int)(cell / L.n2), j = (int)(cell % L.n2);
-    u[L.at(f, i, j)] = (T)src[k];
-  }
-}
-
-template <class T, class H>
-__global__ void gather_kernel(H *dst, const T *u, const Layout L, int i0, int nrows)
-{
-  const long long n = (long long)nrows * L.n2 * NV;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-    const int f = (int)(k % NV);
-    const long long cell = k / NV;
-    const int i = i0 + (int)(cell / L.n2), j = (int)(cell % L.n2);
-    dst[k] = (H)u[L.at(f, i, j)];
-  }
 }
 
 // getdt's reduction in FP64: max over cells of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
@@ -562,32 +542,6 @@ cudaError_t launch_fill(int storage, void *p, size_t count, double value, cudaSt
   if (storage == ST_F32) fill_kernel<float><<<g, 256, 0, s>>>((float *)p, count, (float)value);
   else if (storage == ST_F64) fill_kernel<double><<<g, 256, 0, s>>>((double *)p, count, value);
   else return cudaErrorInvalidValue;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_scatter(int storage, void *u, const void *src, bool host_double, const Layout &L, int i0,
-                           int nrows, cudaStream_t s)
-{
-  const int g = grid_for((long long)nrows * L.n2 * NV, 256);
-  if (storage == ST_F32 && !host_double)
-    scatter_kernel<float, float><<<g, 256, 0, s>>>((float *)u, (const float *)src, L, i0, nrows);
-  else if (storage == ST_F64 && host_double)
-    scatter_kernel<double, double><<<g, 256, 0, s>>>((double *)u, (const double *)src, L, i0, nrows);
-  else
-    return cudaErrorInvalidValue;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_gather(int storage, void *dst, const void *u, bool host_double, const Layout &L, int i0,
-                          int nrows, cudaStream_t s)
-{
-  const int g = grid_for((long long)nrows * L.n2 * NV, 256);
-  if (storage == ST_F32 && !host_double)
-    gather_kernel<float, float><<<g, 256, 0, s>>>((float *)dst, (const float *)u, L, i0, nrows);
-  else if (storage == ST_F64 && host_double)
-    gather_kernel<double, double><<<g, 256, 0, s>>>((double *)dst, (const double *)u, L, i0, nrows);
-  else
-    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

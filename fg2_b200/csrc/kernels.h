@@ -60,12 +60,6 @@ cudaError_t launch_drift(int storage, void *u, const void *v, const Layout &L, d
 cudaError_t launch_euler(int storage, void *u, const Layout &L, double dt, const double *para, double delta1,
                          double delta2, float r1, float r2, cudaStream_t s);
 cudaError_t launch_fill(int storage, void *p, size_t count, double value, cudaStream_t s);
-// host-layout rows [i0, i0 + nrows) (cell-interleaved, `host_double` selects double or
-// float elements) <-> the device layout
-cudaError_t launch_scatter(int storage, void *u, const void *src, bool host_double, const Layout &L, int i0,
-                           int nrows, cudaStream_t s);
-cudaError_t launch_gather(int storage, void *dst, const void *u, bool host_double, const Layout &L, int i0,
-                          int nrows, cudaStream_t s);
 // max over the interior of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2, in double, as
 // an atomic max into status->smax
 cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const double *para, double delta1,

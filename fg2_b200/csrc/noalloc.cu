@@ -112,8 +112,8 @@ int scratch_address(double **out)
 }  // namespace
 }  // namespace fg2
 
-extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, long long plane, int storage,
-                                double *out, void *stream)
+extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, int storage, double *out,
+                                void *stream)
 {
   using namespace fg2;
   if (!u || !out) return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: null array");
@@ -121,9 +121,9 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
   if (n1 > NOALLOC_MAX_ROWS)
     return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: n1 = %d rows exceeds the scratch limit of %d rows", n1,
                      NOALLOC_MAX_ROWS);
-  // pitch = row stride, plane = field stride (element (f, i, j) at f * plane + (i + 3) * pitch + j + 4)
-  if (plane < (long long)n2 + 2 * GL || pitch < (long long)scheme::NVAR * plane)
-    return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: pitch/plane too small for %d x %d", n1, n2);
+  // pitch = row stride (element (f, i, j) at (i + 3) * pitch + (j + 4) * NVAR + f)
+  if (pitch < ((long long)n2 + 2 * GL) * scheme::NVAR)
+    return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: pitch %lld too small for %d x %d", pitch, n1, n2);
   if (storage != ST_F32 && storage != ST_F64)
     return set_error(FG2_ERR_UNSUPPORTED, "fg2_sums_noalloc: storage %d not supported", storage);
   double *scratch = nullptr;
@@ -133,7 +133,7 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
   L.n1 = n1;
   L.n2 = n2;
   L.RS = pitch;
-  L.FS = plane;
+  L.CS = scheme::NVAR;
   cudaStream_t s = (cudaStream_t)stream;
   if (storage == ST_F32) row_sums_kernel<float><<<n1, NA_THREADS, 0, s>>>((const float *)u, L, scratch);
   else row_sums_kernel<double><<<n1, NA_THREADS, 0, s>>>((const double *)u, L, scratch);

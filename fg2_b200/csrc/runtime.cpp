@@ -225,28 +225,18 @@ int read_status(fg2_sim *s)
   return FG2_OK;
 }
 
-// host array (rows of n2 cells x NVAR values) <-> device layout, staged through the
-// spare ping-pong array (dead between steps) in row chunks.
+// host array (rows of n2 cells x NVAR values) <-> device layout.  The device rows hold the
+// same interleaved cells as the host rows, so a transfer is one strided 2D copy.
 int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
 {
-  const size_t hrow = (size_t)s->n2 * scheme::NVAR * host_elem(s->storage);
-  const size_t cap = array_elems(s) * elem_size(s->storage);
-  const int rows_per = (int)std::min<size_t>((size_t)s->n1, cap / hrow);
-  if (rows_per < 1) return fail(FG2_ERR_ARG, "staging buffer too small");
-  void *stage = s->u[1 - s->cur];
-  if (dev_array == stage) return fail(FG2_ERR_ARG, "cannot stage through the target array");
-  const bool hd = s->storage == ST_F64;
-  for (int i0 = 0; i0 < s->n1; i0 += rows_per) {
-    const int nr = std::min(rows_per, s->n1 - i0);
-    char *h = (char *)host + (size_t)i0 * hrow;
-    if (to_device) {
-      CK(cudaMemcpyAsync(stage, h, nr * hrow, cudaMemcpyHostToDevice, s->stream));
-      CK(launch_scatter(s->storage, dev_array, stage, hd, s->L, i0, nr, s->stream));
-    } else {
-      CK(launch_gather(s->storage, stage, dev_array, hd, s->L, i0, nr, s->stream));
-      CK(cudaMemcpyAsync(h, stage, nr * hrow, cudaMemcpyDeviceToHost, s->stream));
-    }
-  }
+  const size_t elem = elem_size(s->storage);
+  if (host_elem(s->storage) != elem) return fail(FG2_ERR_UNSUPPORTED, "storage %d has no host transfer", s->storage);
+  const size_t hrow = (size_t)s->n2 * scheme::NVAR * elem, drow = (size_t)s->L.RS * elem;
+  char *d0 = (char *)dev_array + (size_t)s->L.at(0, 0, 0) * elem;
+  if (to_device)
+    CK(cudaMemcpy2DAsync(d0, drow, host, hrow, hrow, (size_t)s->n1, cudaMemcpyHostToDevice, s->stream));
+  else
+    CK(cudaMemcpy2DAsync(host, hrow, d0, drow, hrow, (size_t)s->n1, cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return FG2_OK;
 }
@@ -304,7 +294,7 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   s->n1 = n1;
   s->n2 = n2;
   s->storage = storage;
-  s->L = make_layout(n1, n2, scheme::NVAR, elem_size(storage));
+  s->L = make_layout(n1, n2, scheme::NVAR);
   for (int q = 0; q < NPARA; ++q) s->para[q] = 0.0;
   for (int q = 0; q < scheme::NSLOT; ++q) s->para[scheme::PARA_KEYS[q].slot] = round_para(s.get(), scheme::PARA_KEYS[q].def);
   scheme::derive(s->para);
@@ -720,11 +710,11 @@ void *fg2_sim_u(fg2_sim *s) { return s ? s->u[s->cur] : nullptr; }
 void *fg2_sim_v(fg2_sim *s) { return s ? s->v : nullptr; }
 void *fg2_sim_stream(fg2_sim *s) { return s ? (void *)s->stream : nullptr; }
 
-int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane)
+int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *cell)
 {
   if (!s) return fail(FG2_ERR_ARG, "null handle");
   if (pitch) *pitch = s->L.RS;
-  if (plane) *plane = s->L.FS;
+  if (cell) *cell = s->L.CS;
   return FG2_OK;
 }
 

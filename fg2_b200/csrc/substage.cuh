@@ -8,8 +8,9 @@
 //
 // Data movement.  u streams through a ring of NSLOT shared-memory slots by TMA
 // (cp.async.bulk.tensor.3d, no multicast): chunk 0 of a tile is the 7-row warm-up box
-// u[i0-4 .. i0+3) x [j0-4, j0+132) (all fields), chunk b+1 the 7 leading rows u[i0+3+7b ..]
-// of output block b; a box lands as [row][field][column].  When a block's u chunk is
+// u[i0-4 .. i0+3) x [j0-4, j0+132), chunk b+1 the 7 leading rows u[i0+3+7b ..] of output
+// block b; a box lands as [row][cell][field], the cells' fields interleaved as in HBM, so a
+// thread reads a whole hydro cell with one 16-byte shared load.  When a block's u chunk is
 // issued, the same 7 rows of v are prefetched into L2 (cp.async.bulk.prefetch.tensor), and
 // each thread loads its v values a row before it needs them.  The block's results (u' and
 // the new v) are staged in shared memory and written back with one TMA tensor store per
@@ -20,7 +21,7 @@
 // timeout before leaving, which raises an error bit in the status block.
 //
 // Stencil.  Each thread walks its column down the tile.  At every leading row L it loads the
-// 7 values u(L, j-3..j+3) of each field from shared memory and computes the axis-2
+// 7 cells u(L, j-3..j+3) from shared memory and computes the axis-2
 // (contiguous) derivatives D2 and D22 of row L, pushes u(L, j) into a 7-row register window
 // (the axis-1 stencil of row L-3 then needs no further loads), and feeds the mixed
 // derivative by streaming accumulators: with delta_k(r) = u(r, j+k) - u(r, j-k),
@@ -58,6 +59,7 @@ static_assert(scheme::U1 == 1 && scheme::U2 == 2, "u1 and u2 are fields 1 and 2"
 template <class T>
 struct Geo {
   static constexpr int NSLOT = sizeof(T) == 8 ? 2 : FG2_NSLOT_F32;
+  static constexpr int G = 16 / (int)sizeof(T);  // cells per 16-byte group (TMA box unit)
   static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * NV * sizeof(T));
   static constexpr uint32_t SLOT = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
   static constexpr uint32_t OUT_BYTES = (uint32_t)(SW * CH * NV * sizeof(T));  // one block of one array
@@ -66,9 +68,62 @@ struct Geo {
   // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], producer state
   static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + NSLOT * sizeof(int) + 4 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0 && OUT_BYTES % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
-  static_assert(BW <= 256 && CH <= 256, "TMA box dimensions");
-  static_assert((BW * sizeof(T)) % 16 == 0 && (SW * sizeof(T)) % 16 == 0, "TMA rows must be 16-byte multiples");
+  static_assert(BW % G == 0 && SW % G == 0 && GL % G == 0, "boxes and tile origins are whole cell groups");
+  static_assert(BW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
 };
+
+// One cell's NV values as field pairs ((lnd, u1), (u2, lne)): one or two 16-byte accesses for
+// a hydro cell, scalar ones for a 3-field cell.  The _cs forms stream through the caches.
+template <class T>
+__device__ __forceinline__ void ld_cell(const T *p, typename PairOf<T>::type out[NP])
+{
+  using PO = PairOf<T>;
+  if constexpr (NV == 4 && sizeof(T) == 4) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    out[0] = make_float2(x.x, x.y);
+    out[1] = make_float2(x.z, x.w);
+  } else if constexpr (NV == 4 && sizeof(T) == 8) {
+    out[0] = *reinterpret_cast<const double2 *>(p);
+    out[1] = *reinterpret_cast<const double2 *>(p + 2);
+  } else {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) out[q] = PO::make(p[2 * q], 2 * q + 1 < NV ? p[2 * q + 1] : T(0));
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void ld_cell_cs(const T *p, typename PairOf<T>::type out[NP])
+{
+  using PO = PairOf<T>;
+  if constexpr (NV == 4 && sizeof(T) == 4) {
+    const float4 x = __ldcs(reinterpret_cast<const float4 *>(p));
+    out[0] = make_float2(x.x, x.y);
+    out[1] = make_float2(x.z, x.w);
+  } else if constexpr (NV == 4 && sizeof(T) == 8) {
+    out[0] = __ldcs(reinterpret_cast<const double2 *>(p));
+    out[1] = __ldcs(reinterpret_cast<const double2 *>(p + 2));
+  } else {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) out[q] = PO::make(__ldcs(p + 2 * q), 2 * q + 1 < NV ? __ldcs(p + 2 * q + 1) : T(0));
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void st_cell(T *p, const typename PairOf<T>::type in[NP])
+{
+  if constexpr (NV == 4 && sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(in[0].x, in[0].y, in[1].x, in[1].y);
+  } else if constexpr (NV == 4 && sizeof(T) == 8) {
+    *reinterpret_cast<double2 *>(p) = in[0];
+    *reinterpret_cast<double2 *>(p + 2) = in[1];
+  } else {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      p[2 * q] = in[q].x;
+      if (2 * q + 1 < NV) p[2 * q + 1] = in[q].y;
+    }
+  }
+}
 
 // Tile t of a single grid: strip fastest, so horizontally adjacent tiles run together and
 // share their halo columns through L2.
@@ -114,20 +169,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Leading-row work of field pair PI for register slot R.
+// Leading-row work of field pair PI for register slot R, from the pair's values at
+// columns j-3 .. j+3 of the leading row.
 template <class T, unsigned M2, int R, int PI>
-__device__ __forceinline__ void lead_pair(const T *row, const KParams<T> &a, Roll<T> &s,
+__device__ __forceinline__ void lead_pair(const typename PairOf<T>::type (&x)[7][NP], const KParams<T> &a, Roll<T> &s,
                                           typename PairOf<T>::type dk[3])
 {
   using P = typename PairOf<T>::type;
-  using PO = PairOf<T>;
-  constexpr bool two = 2 * PI + 1 < NV;
-  const T *q0 = row + (2 * PI) * BW;
-  const T *q1 = q0 + BW;
-  const P c = PO::make(q0[0], two ? q1[0] : T(0));
-  const P l1 = PO::make(q0[-1], two ? q1[-1] : T(0)), r1 = PO::make(q0[1], two ? q1[1] : T(0));
-  const P l2 = PO::make(q0[-2], two ? q1[-2] : T(0)), r2 = PO::make(q0[2], two ? q1[2] : T(0));
-  const P l3 = PO::make(q0[-3], two ? q1[-3] : T(0)), r3 = PO::make(q0[3], two ? q1[3] : T(0));
+  const P l3 = x[0][PI], l2 = x[1][PI], l1 = x[2][PI], c = x[3][PI], r1 = x[4][PI], r2 = x[5][PI], r3 = x[6][PI];
   s.w[PI][R] = c;
   dk[0] = r1 - l1;
   dk[1] = r2 - l2;
@@ -145,15 +194,19 @@ __device__ __forceinline__ void lead_pair(const T *row, const KParams<T> &a, Rol
   }
 }
 
-// Leading-row work for register slot R: loads row R of the chunk.
+// Leading-row work for register slot R: loads the 7 cells of row R of the chunk around the
+// thread's column.
 template <class T, unsigned M2, int R>
 __device__ __forceinline__ void lead_row(const T *su, int tx, const KParams<T> &a, Roll<T> &s)
 {
   using P = typename PairOf<T>::type;
-  const T *row = su + R * (NV * BW) + tx + GL;
+  const T *row = su + (R * BW + tx + GL - 3) * NV;
+  P x[7][NP];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) ld_cell<T>(row + k * NV, x[k]);
   P dk[NP][3];
-  lead_pair<T, M2, R, 0>(row, a, s, dk[0]);
-  if constexpr (NP > 1) lead_pair<T, M2, R, 1>(row, a, s, dk[1]);
+  lead_pair<T, M2, R, 0>(x, a, s, dk[0]);
+  if constexpr (NP > 1) lead_pair<T, M2, R, 1>(x, a, s, dk[1]);
   // D12 of u1 (pair 0, lane y) and u2 (pair 1, lane x): rows L+k get -m_k delta_k(L) (mn = -m),
   // rows L-k get +m_k delta_k(L); row L-3 is then complete.  The first contribution to row
   // L+3 initialises its accumulator.
@@ -176,13 +229,13 @@ template <class T, bool READ_V>
 __device__ __forceinline__ void load_v(const T *v, const Layout &L, int i, int j, bool ok,
                                        typename PairOf<T>::type vr[NP])
 {
+  using P = typename PairOf<T>::type;
   if (!READ_V) return;
-  ok = ok && i < L.n1 && j < L.n2;
-  const T *q = v + L.at(0, i, j);
+  if (ok && i < L.n1 && j < L.n2) {
+    ld_cell_cs<T>(v + L.at(0, i, j), vr);
+  } else {
 #pragma unroll
-  for (int p = 0; p < NP; ++p) {
-    vr[p].x = ok ? __ldcs(q + (2 * p) * L.FS) : T(0);
-    vr[p].y = (ok && 2 * p + 1 < NV) ? __ldcs(q + (2 * p + 1) * L.FS) : T(0);
+    for (int p = 0; p < NP; ++p) vr[p] = lit<P>(0.0);
   }
 }
 
@@ -224,7 +277,7 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const Roll<T> &s,
 }
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
-// Results go to the block's staging buffers (rows [R][field][column]); edge cells also write
+// Results go to the block's staging buffers (rows [R][cell][field]); edge cells also write
 // their ghost images to u_out.
 template <class T, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
 __device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], int i, int j, int tx,
@@ -243,34 +296,26 @@ __device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], 
 
   T r[NV];
   scheme::eqns<M2>(cell, a.p, i, j, r, a.ks.delta1);
-  T qn[NV];
+  P vn[NP], qp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
-    const bool two = 2 * p + 1 < NV;
-    P vn = PairOf<T>::make(r[2 * p], two ? r[2 * p + 1] : T(0));
-    if (READ_V) vn = fmac(a.beta2, vr[p], vn);
-    const P qp = fmac(gdt2, vn, PairOf<T>::make(cell.q[2 * p], two ? cell.q[2 * p + 1] : T(0)));
-    if (WRITE_V) {
-      stage_v[(R * NV + 2 * p) * SW + tx] = vn.x;
-      if (two) stage_v[(R * NV + 2 * p + 1) * SW + tx] = vn.y;
-    }
-    qn[2 * p] = qp.x;
-    if (two) qn[2 * p + 1] = qp.y;
+    vn[p] = PairOf<T>::make(r[2 * p], 2 * p + 1 < NV ? r[2 * p + 1] : T(0));
+    if (READ_V) vn[p] = fmac(a.beta2, vr[p], vn[p]);
+    qp[p] = fmac(gdt2, vn[p], s.w[p][S0]);
   }
-  if (WRITE_U) {
-#pragma unroll
-    for (int f = 0; f < NV; ++f) stage_u[(R * NV + f) * SW + tx] = qn[f];
-  }
+  const int so = (R * SW + tx) * NV;
+  if (WRITE_V) st_cell<T>(stage_v + so, vn);
+  if (WRITE_U) st_cell<T>(stage_u + so, qp);
   if (i >= L.n1 || j >= L.n2) return;  // cells past the grid: staged values are clipped by the store
+  T qn[NV];
+#pragma unroll
+  for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
 #pragma unroll
   for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
-  if (j >= a.store_cols) {  // interior columns past the bulk stores' last whole 16-byte chunk
+  if (j >= a.store_cols) {  // interior columns past the bulk stores' last whole cell group
     const long long o = L.at(0, i, j);
-#pragma unroll
-    for (int f = 0; f < NV; ++f) {
-      if (WRITE_U) u_out[o + f * L.FS] = qn[f];
-      if (WRITE_V) v[o + f * L.FS] = stage_v[(R * NV + f) * SW + tx];
-    }
+    if (WRITE_U) st_cell<T>(u_out + o, qp);
+    if (WRITE_V) st_cell<T>(v + o, vn);
   }
   if (WRITE_U) store_ghosts<T, T>(u_out, L, i, j, qn, a.p1, a.p2);
   if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, a.ks));
@@ -306,10 +351,11 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     const int i0 = (ps->tile / tg.strips) * TH, j0 = (ps->tile % tg.strips) * SW;
     const int c = ps->c;
     mbar_arrive_expect_tx(&full[s], G::U_BYTES);
-    // box coordinates (padded column, field, padded row): rows i0 - 4 + 7c .., columns j0 - 4 ..
-    tma_load_3d(smem + (size_t)s * G::SLOT, tm_u, &full[s], j0, 0, i0 - 4 + CH * c + GT);
+    // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
+    // columns j0 - 4 .. (padded column j0)
+    tma_load_3d(smem + (size_t)s * G::SLOT, tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
     // the v rows this chunk's output block updates, into L2 ahead of the threads' loads
-    if (READ_V && c > 0) tma_prefetch_l2_3d(tm_v, j0 + GL, 0, i0 + CH * (c - 1) + GT);
+    if (READ_V && c > 0) tma_prefetch_l2_3d(tm_v, 0, (j0 + GL) / G::G, i0 + CH * (c - 1) + GT);
     ps->c = c == NB ? 0 : c + 1;
   }
   ps->next_n = n + 1;
@@ -408,8 +454,8 @@ __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid
       if (b >= 0 && i0 + CH * b < L.n1) {
         // interior rows ib .. ib+6 of the strip; the maps clip at the last interior row/column
         const int ib = i0 + CH * b;
-        if (WRITE_U) tma_store_3d(&tm_uo, stage_u, j0 + GL, 0, ib + GT);
-        if (WRITE_V) tma_store_3d(&tm_vo, stage_v, j0 + GL, 0, ib + GT);
+        if (WRITE_U) tma_store_3d(&tm_uo, stage_u, 0, (j0 + GL) / G::G, ib + GT);
+        if (WRITE_V) tma_store_3d(&tm_vo, stage_v, 0, (j0 + GL) / G::G, ib + GT);
         if (WRITE_U || WRITE_V) bulk_commit();
       }
       issue_chunk<T, READ_V>(ps, smem, full, tile_of, &tm_u, &tm_v, queue, tg);  // refill slot s

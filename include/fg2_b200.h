@@ -125,11 +125,12 @@ int fg2_sim_seed_forcing(fg2_sim *s, uint64_t seed);
  * reduction order (bitwise reproducible). */
 int fg2_sim_sums(fg2_sim *s, double out[4]);
 /* Current device arrays and their layout: element (f, i, j) at
- * base[f * plane + (i + 3) * pitch + (j + 4)], elements of the storage type; pitch is the
- * stride of a grid row (all NVAR field rows of it), plane the stride between fields. */
+ * base[(i + 3) * pitch + (j + 4) * cell + f], elements of the storage type; cells hold their
+ * NVAR fields interleaved as in the host layout (cell = NVAR), pitch is the stride of a grid
+ * row (a multiple of 32 cells, every row 128-byte aligned). */
 void *fg2_sim_u(fg2_sim *s);
 void *fg2_sim_v(fg2_sim *s);
-int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *plane);
+int fg2_sim_layout(const fg2_sim *s, long long *pitch, long long *cell);
 void *fg2_sim_stream(fg2_sim *s);
 /* dump()/load() (src/io.cpp:24-76): the reference's .raw frame format. */
 int fg2_sim_dump(fg2_sim *s, const char *path, double time);
@@ -147,7 +148,7 @@ int fg2_sim_load(fg2_sim *s, const char *path, double *time);
  * device looks up the array's device address; make it before any stream capture.
  * Enqueued on `stream` without synchronising. */
 #define FG2_NOALLOC_MAX_ROWS 16384
-int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, long long plane, int storage, double *out,
+int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, int storage, double *out,
                      void *stream);
 
 /* ---- reference-mirror API (src/fg2.h:60-84) over one process-wide simulation ------------ */

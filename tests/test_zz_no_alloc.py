@@ -26,10 +26,11 @@ def test_sums_noalloc_matches_allocating_sums(scheme, storage, n1, n2, cuda):
         for s, seed in ((a, 11), (b, 12)):
             s.config()
             s.init("turb" if scheme == "hydro-isot" else "kh", seed=seed)
-        pitch, plane = a.layout()
+        pitch, cell = a.layout()
+        assert cell == a.nvar
         for sim in (a, b, a):  # calls in a row, on different states, reusing the static scratch
             expect = sim.sums()
-            rc = lib.fg2_sums_noalloc(lib.fg2_sim_u(sim.h), n1, n2, pitch, plane, fg2_b200.STORAGE[storage],
+            rc = lib.fg2_sums_noalloc(lib.fg2_sim_u(sim.h), n1, n2, pitch, fg2_b200.STORAGE[storage],
                                       out.data_ptr(), sim.stream)
             assert rc == 0, lib.fg2_last_error()
             torch.cuda.synchronize()
@@ -41,8 +42,8 @@ def test_sums_noalloc_rejects_grids_beyond_the_scratch(cuda):
     lib = fg2_b200.load_library("hydro")
     out = torch.zeros(4, dtype=torch.float64, device=cuda)
     with fg2_b200.Sim(16, 16) as s:
-        pitch, plane = s.layout()
+        pitch, _ = s.layout()
         # rejected on the host before anything is launched
-        too_many = lib.fg2_sums_noalloc(lib.fg2_sim_u(s.h), 20000, 16, pitch, plane, 0, out.data_ptr(), s.stream)
+        too_many = lib.fg2_sums_noalloc(lib.fg2_sim_u(s.h), 20000, 16, pitch, 0, out.data_ptr(), s.stream)
     assert too_many == -1
     assert b"exceeds the scratch limit" in lib.fg2_last_error()
