@@ -57,11 +57,9 @@ struct KParams {
   Coef<T> ks;  // scalar stencil weights
   Para<T> p;   // scheme parameters
   P beta2;     // the stage's beta on both lanes
-  int store_cols;  // interior columns the bulk stores cover (the rest are stored per thread)
   double gamma, dt;
-  const double *dt_dev;
-  int p1, p2;
-  Status *status;
+  const double *dt_dev;  // device time step for grids without their own, or null: dt
+  Status *status;        // launch errors
 };
 
 template <class T>
@@ -70,13 +68,14 @@ static typename PairOf<T>::type bc(double x)
   return PairOf<T>::make((T)x, (T)x);
 }
 
+// scaled: plain weights (Delta = 1), the grids' 1/Delta factors are applied in the kernel.
 template <class T>
-static KParams<T> make_params(const StageArgs &a)
+static KParams<T> make_params(const StageArgs &a, bool scaled)
 {
   KParams<T> kp;
   // Delta = l / n is rounded to the state precision (src/config.cpp:39); the weights are
   // divided by it in double and rounded once.
-  const double d1 = a.delta1, d2 = a.delta2;
+  const double d1 = scaled ? 1.0 : a.delta1, d2 = scaled ? 1.0 : a.delta2;
   const double w1[3] = {45. / 60., -9. / 60., 1. / 60.};
   const double w2[4] = {-490. / 180., 270. / 180., -27. / 180., 2. / 180.};
   const double wm[3] = {270. / 720., -27. / 720., 2. / 720.};
@@ -111,11 +110,8 @@ static KParams<T> make_params(const StageArgs &a)
   for (int q = 0; q < NPARA; ++q) kp.p.v[q] = (T)(a.para ? a.para[q] : 0.0);
   kp.beta2 = bc<T>(a.beta);
   kp.gamma = a.gamma;
-  kp.store_cols = a.store_cols;
   kp.dt = a.dt;
   kp.dt_dev = a.dt_dev;
-  kp.p1 = a.p1;
-  kp.p2 = a.p2;
   kp.status = a.status;
   return kp;
 }
@@ -183,10 +179,10 @@ __device__ __forceinline__ void store_images(T *u, const Layout &L, int i, int j
 }
 
 template <class C>
-__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, const Coef<C> &k)
+__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2)
 {
   const C cs = scheme::sound_speed(q, p);
-  return fmac(vabs(q[scheme::U1]) + cs, k.inv1, (vabs(q[scheme::U2]) + cs) * k.inv2);
+  return fmac(vabs(q[scheme::U1]) + cs, inv1, (vabs(q[scheme::U2]) + cs) * inv2);
 }
 
 #include "substage.cuh"
@@ -194,6 +190,7 @@ __device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, const Coe
 // ---------------------------------------------------------------------------------------
 // Tensor maps: u with the halo box of one chunk, v with the interior box of one chunk.
 namespace {
+static_assert(sizeof(GridDesc) % 64 == 0 && alignof(GridDesc) == 64, "grid descriptors keep tensor-map alignment");
 PFN_cuTensorMapEncodeTiled_v12000 encoder()
 {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -235,41 +232,39 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
 }
 }  // namespace
 
-CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
+CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
+                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0)
 {
-  return encode_map(map, base, L, storage, sub::BW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
-}
-
-CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
-{
-  return encode_map(map, base, L, storage, sub::SW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
-}
-
-// Interior columns a bulk store may write: a store clips a box at the map's extent only at
-// whole cell groups, so the store map ends at the last group that lies entirely inside the
-// interior; the (fewer than one group of) interior columns after it are stored by their
-// threads.
-int store_cols(const Layout &L, int storage)
-{
-  const int G = group_cells(storage);
-  return (L.n2 + GL) / G * G - GL;
-}
-
-// Store map: ends at the last interior row (padded n1 + GT - 1) and at column store_cols - 1,
-// so a bulk store of a partial tile writes no ghost cell.
-CUresult encode_store_map(CUtensorMap *map, const void *base, const Layout &L, int storage)
-{
-  return encode_map(map, base, L, storage, sub::SW, sub::CH, store_cols(L, storage) + GL, L.n1 + GT);
+  CUresult r = encode_map(&d->tm_u, u_in, L, storage, sub::BW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+  if (r != CUDA_SUCCESS) return r;
+  r = encode_map(&d->tm_v, v, L, storage, sub::SW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+  if (r != CUDA_SUCCESS) return r;
+  d->u_out = u_out;
+  d->v = v;
+  d->L = L;
+  d->strips = sub::tile_grid(L).strips;
+  d->tile0 = tile0;
+  d->p1 = p1;
+  d->p2 = p2;
+  d->dt = dt;
+  d->status = status;
+  d->inv1 = 1.0 / delta1;
+  d->inv2 = 1.0 / delta2;
+  d->inv11 = 1.0 / (delta1 * delta1);
+  d->inv22 = 1.0 / (delta2 * delta2);
+  d->inv12 = 1.0 / (delta1 * delta2);
+  d->delta1 = delta1;
+  return CUDA_SUCCESS;
 }
 
 int substage_tiles(const Layout &L) { return sub::tile_grid(L).ntiles; }
 
-template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF>
-static cudaError_t run_substage(const StageMaps &m, T *u_out, T *v, const Layout &L, const KParams<T> &kp, int *queue,
+template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
+static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<T> &kp, int *queue,
                                 cudaStream_t s)
 {
-  using G = sub::Geo<T>;
-  auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF>;
+  using G = sub::Geo<T, RV>;
+  auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF, SC>;
   static int ctas_per_sm = 0, sms = 0;
   if (!ctas_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
@@ -281,24 +276,24 @@ static cudaError_t run_substage(const StageMaps &m, T *u_out, T *v, const Layout
       return e;
     if (ctas_per_sm < 1) return cudaErrorInvalidConfiguration;
   }
-  const int ntiles = sub::tile_grid(L).ntiles;
+  if (ntiles < 1) return cudaSuccess;
   int grid = sms * ctas_per_sm;
   if (grid > ntiles) grid = ntiles;
-  kern<<<grid, sub::NT, G::SMEM, s>>>(*m.u_in, *m.v_in, *m.u_out, *m.v_out, u_out, v, L, kp, queue);
+  kern<<<grid, sub::NT, G::SMEM, s>>>(grids, ngrids, ntiles, kp, queue);
   return cudaGetLastError();
 }
 
-template <class T, unsigned M2>
-static cudaError_t substage_m(int kind, bool cfl, const StageMaps &m, T *uo, T *vv, const Layout &L,
-                              const KParams<T> &kp, int *queue, cudaStream_t s)
+template <class T, unsigned M2, bool SC>
+static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int nt, const KParams<T> &kp, int *queue,
+                              cudaStream_t s)
 {
   switch (kind) {
-    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false>(m, uo, vv, L, kp, queue, s);
-    case STAGE_MID: return run_substage<T, M2, true, true, true, false>(m, uo, vv, L, kp, queue, s);
+    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false, SC>(g, ng, nt, kp, queue, s);
+    case STAGE_MID: return run_substage<T, M2, true, true, true, false, SC>(g, ng, nt, kp, queue, s);
     case STAGE_LAST:
-      return cfl ? run_substage<T, M2, true, false, true, true>(m, uo, vv, L, kp, queue, s)
-                 : run_substage<T, M2, true, false, true, false>(m, uo, vv, L, kp, queue, s);
-    case STAGE_KICK: return run_substage<T, M2, true, true, false, false>(m, uo, vv, L, kp, queue, s);
+      return cfl ? run_substage<T, M2, true, false, true, true, SC>(g, ng, nt, kp, queue, s)
+                 : run_substage<T, M2, true, false, true, false, SC>(g, ng, nt, kp, queue, s);
+    case STAGE_KICK: return run_substage<T, M2, true, true, false, false, SC>(g, ng, nt, kp, queue, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -306,25 +301,27 @@ static cudaError_t substage_m(int kind, bool cfl, const StageMaps &m, T *uo, T *
 // The kernels are compiled for two sets of second-derivative fields: the scheme's default
 // parameters' set, and all fields (correct for any parameters: an unused D11/D22 meets a
 // zero coefficient).  FP64, the reference-precision path, always uses all fields.
-template <class T>
-static cudaError_t substage_t(int kind, bool cfl, const StageMaps &m, void *u_out, void *v, const Layout &L,
-                              const StageArgs &a, int *queue, cudaStream_t s)
+template <class T, bool SC>
+static cudaError_t substage_t(int kind, bool cfl, const GridDesc *g, int ng, int nt, const StageArgs &a, int *queue,
+                              cudaStream_t s)
 {
-  const KParams<T> kp = make_params<T>(a);
-  T *uo = (T *)u_out, *vv = (T *)v;
+  const KParams<T> kp = make_params<T>(a, SC);
   const unsigned need = scheme::d2_fields(a.para);
   if constexpr (sizeof(T) == 4) {
-    if ((need & ~scheme::D2_DEFAULT) == 0)
-      return substage_m<T, scheme::D2_DEFAULT>(kind, cfl, m, uo, vv, L, kp, queue, s);
+    if ((need & ~scheme::D2_DEFAULT) == 0) return substage_m<T, scheme::D2_DEFAULT, SC>(kind, cfl, g, ng, nt, kp, queue, s);
   }
-  return substage_m<T, scheme::D2_ALL>(kind, cfl, m, uo, vv, L, kp, queue, s);
+  return substage_m<T, scheme::D2_ALL, SC>(kind, cfl, g, ng, nt, kp, queue, s);
 }
 
-cudaError_t launch_substage(int storage, int kind, bool cfl, const StageMaps &m, void *u_out, void *v, const Layout &L,
-                            const StageArgs &a, int *queue, cudaStream_t s)
+cudaError_t launch_substage(int storage, int kind, bool cfl, bool scaled, const GridDesc *grids, int ngrids,
+                            int ntiles, const StageArgs &a, int *queue, cudaStream_t s)
 {
-  if (storage == ST_F32) return substage_t<float>(kind, cfl, m, u_out, v, L, a, queue, s);
-  if (storage == ST_F64) return substage_t<double>(kind, cfl, m, u_out, v, L, a, queue, s);
+  if (storage == ST_F32)
+    return scaled ? substage_t<float, true>(kind, cfl, grids, ngrids, ntiles, a, queue, s)
+                  : substage_t<float, false>(kind, cfl, grids, ngrids, ntiles, a, queue, s);
+  if (storage == ST_F64)
+    return scaled ? substage_t<double, true>(kind, cfl, grids, ngrids, ntiles, a, queue, s)
+                  : substage_t<double, false>(kind, cfl, grids, ngrids, ntiles, a, queue, s);
   return cudaErrorInvalidValue;
 }
 

@@ -23,8 +23,7 @@ struct StageArgs {
   double delta1, delta2;
   const double *para;   // scheme parameters by slot
   int p1, p2;           // boundary kind per axis (BC_PERIODIC / BC_WALL)
-  Status *status;       // device status block
-  int store_cols;       // interior columns covered by the bulk-store maps (store_cols())
+  Status *status;       // device status block (launch errors; per-grid blocks are in GridDesc)
 };
 
 enum StageKind : int {
@@ -34,25 +33,37 @@ enum StageKind : int {
   STAGE_KICK = 3,   // the reference's kick(): v <- F(u) + beta v only, u untouched
 };
 
-// Tensor maps over one state array (all fields) in the device layout: u with the halo box
-// of one row chunk of the fused substage kernel, v with its interior box, and the store map
-// (interior box, extents ending at the interior) that bulk stores write through.  Return
-// CUDA_SUCCESS or the driver's error.
-CUresult encode_u_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
-CUresult encode_v_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
-CUresult encode_store_map(CUtensorMap *map, const void *base, const Layout &L, int storage);
-int store_cols(const Layout &L, int storage);
-int substage_tiles(const Layout &L);
-
-// The four maps one substage launch uses: u read (halo box), v prefetched, u' stored, v stored.
-struct StageMaps {
-  const CUtensorMap *u_in, *v_in, *u_out, *v_out;
+// One grid of a substage launch, in device memory (the tensor maps keep CUtensorMap's
+// 64-byte alignment).  A launch advances a list of grids in tile order: grid k owns launch
+// tiles [tile0_k, tile0_k + tiles of grid k).
+struct GridDesc {
+  CUtensorMap tm_u;       // u (input): 7-row halo boxes of a strip
+  CUtensorMap tm_v;       // v: 7-row interior boxes of a strip
+  void *u_out;            // u' (written stages)
+  void *v;                // v (read and/or written)
+  Layout L;
+  int strips;             // tile columns of this grid
+  int tile0;              // its first launch tile
+  int p1, p2;             // boundary kind per axis (BC_PERIODIC / BC_WALL)
+  const double *dt;       // device time step of this grid, or null: the launch's
+  Status *status;         // NaN flag and CFL max of this grid
+  double inv1, inv2;      // 1 / Delta per axis (batch launches scale by these)
+  double inv11, inv22, inv12;  // 1 / (Delta1 Delta1), 1 / (Delta2 Delta2), 1 / (Delta1 Delta2)
+  double delta1;          // Delta1
 };
 
-// One fused substage over a whole grid.  `queue` is the simulation's tile queue: two ints,
-// zero before the first launch; every launch leaves them zero again.
-cudaError_t launch_substage(int storage, int kind, bool cfl, const StageMaps &maps, void *u_out, void *v,
-                            const Layout &L, const StageArgs &a, int *queue, cudaStream_t s);
+// Fills a GridDesc (tensor maps over u_in and v encoded here).  Returns CUDA_SUCCESS or the
+// driver's error.
+CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
+                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0);
+int substage_tiles(const Layout &L);
+
+// One fused substage over the grids of `grids` (device array of ngrids descriptors holding
+// ntiles tiles in all).  `scaled`: the grids differ in Delta (stencil weights scaled per grid);
+// otherwise a.delta1/a.delta2 are folded into the weights.  `queue` is the launch's tile
+// queue: two ints, zero before the first launch; every launch leaves them zero again.
+cudaError_t launch_substage(int storage, int kind, bool cfl, bool scaled, const GridDesc *grids, int ngrids,
+                            int ntiles, const StageArgs &a, int *queue, cudaStream_t s);
 
 cudaError_t launch_bcond(int storage, void *u, const Layout &L, int p1, int p2, cudaStream_t s);
 cudaError_t launch_drift(int storage, void *u, const void *v, const Layout &L, double dt, Status *status,

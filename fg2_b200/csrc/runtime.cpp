@@ -81,10 +81,10 @@ struct fg2_sim {
   void *u[2] = {nullptr, nullptr};
   void *v = nullptr;
   int cur = 0;  // u[cur] holds the state
-  CUtensorMap map[2];     // u[0], u[1] with the substage kernel's halo box
-  CUtensorMap vmap;       // v with the interior box
-  CUtensorMap omap[2];    // u[0], u[1] store maps (interior)
-  CUtensorMap vomap;      // v store map (interior)
+  // substage descriptors: [0] u[0] -> u[1], [1] u[1] -> u[0], [2] the mirror API's kick
+  GridDesc *desc = nullptr;   // device
+  GridDesc desc_host[3];
+  bool desc_valid = false;
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -105,9 +105,6 @@ struct fg2_sim {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step graph per ping-pong parity
   double graph_dt[2] = {0, 0}, graph_tend[2] = {0, 0};
   char para_msg[256];
-  // the reference-mirror kick/drift may name arbitrary arrays: tensor map cache
-  const void *kick_map_base = nullptr, *kick_vmap_base = nullptr;
-  CUtensorMap kick_map, kick_vmap, kick_vomap;
 };
 
 namespace {
@@ -142,8 +139,29 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p1 = s->p1;
   a.p2 = s->p2;
   a.status = s->status;
-  a.store_cols = store_cols(s->L, s->storage);
   return a;
+}
+
+// The two ping-pong descriptors (boundaries and Delta as configured); uploaded before any
+// capture, since every path that launches a substage calls this first.
+int ensure_descs(fg2_sim *s)
+{
+  if (s->desc_valid) return FG2_OK;
+  for (int k = 0; k < 2; ++k)
+    if (make_grid_desc(&s->desc_host[k], s->u[k], s->u[1 - k], s->v, s->L, s->storage, s->p1, s->p2, s->delta1,
+                       s->delta2, nullptr, s->status, 0) != CUDA_SUCCESS)
+      return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
+  CK(cudaMemcpyAsync(s->desc, s->desc_host, 2 * sizeof(GridDesc), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->desc_valid = true;
+  return FG2_OK;
+}
+
+// One substage of the state u[cur] into u[1 - cur] (kick: v only).
+int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridDesc *desc)
+{
+  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L), a, s->queue, s->stream));
+  return FG2_OK;
 }
 
 bool supported_storage(int st) { return st == ST_F32 || st == ST_F64; }
@@ -187,6 +205,8 @@ bool euler_active(const fg2_sim *s)
 // One RK3 step: Euler hook, three fused substages.  dt_dev != null: device-resident dt.
 int enqueue_step(fg2_sim *s, double dt, const double *dt_dev, bool cfl)
 {
+  int rc0 = ensure_descs(s);
+  if (rc0) return rc0;
   if (euler_active(s)) {
     int rc = do_euler(s, dt);
     if (rc) return rc;
@@ -198,8 +218,8 @@ int enqueue_step(fg2_sim *s, double dt, const double *dt_dev, bool cfl)
   for (int k = 0; k < 3; ++k) {
     const StageArgs a = stage_args(s, k, dt, dt_dev);
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-    const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
-    CK(launch_substage(s->storage, kind, cfl && k == 2, m, s->u[1 - s->cur], s->v, s->L, a, s->queue, s->stream));
+    int rc = launch_stage(s, kind, cfl && k == 2, a, s->desc + s->cur);
+    if (rc) return rc;
     s->cur = 1 - s->cur;
   }
   s->ghosts_valid = true;
@@ -241,8 +261,10 @@ int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
   return FG2_OK;
 }
 
+// Settings changed: the captured graphs and the descriptors are rebuilt on next use.
 void drop_graph(fg2_sim *s)
 {
+  s->desc_valid = false;
   for (int b = 0; b < 2; ++b) {
     if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
     s->graph[b] = nullptr;
@@ -323,16 +345,7 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
       cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess)
     return cleanup("reduction scratch allocation failed");
   if (cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess) return cleanup("queue allocation failed");
-  if (encode_u_map(&s->map[0], s->u[0], s->L, storage) != CUDA_SUCCESS ||
-      encode_u_map(&s->map[1], s->u[1], s->L, storage) != CUDA_SUCCESS ||
-      encode_v_map(&s->vmap, s->v, s->L, storage) != CUDA_SUCCESS ||
-      encode_store_map(&s->omap[0], s->u[0], s->L, storage) != CUDA_SUCCESS ||
-      encode_store_map(&s->omap[1], s->u[1], s->L, storage) != CUDA_SUCCESS ||
-      encode_store_map(&s->vomap, s->v, s->L, storage) != CUDA_SUCCESS) {
-    fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
-    fg2_sim_destroy(s.release());
-    return nullptr;
-  }
+  if (cudaMalloc(&s->desc, 3 * sizeof(GridDesc)) != cudaSuccess) return cleanup("descriptor allocation failed");
   // every array starts at -max like the reference (src/setup.cpp:80-83)
   const double lowest = storage == ST_F64 ? -std::numeric_limits<double>::max() : -std::numeric_limits<float>::max();
   if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
@@ -358,6 +371,7 @@ void fg2_sim_destroy(fg2_sim *s)
   cudaFree(s->sums_partial);
   cudaFree(s->sums_out);
   cudaFree(s->queue);
+  cudaFree(s->desc);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -562,6 +576,8 @@ int fg2_sim_advance_graph(fg2_sim *s, int nsteps, double dt, double t_end)
     --nsteps;
   }
   if (nsteps <= 0) return FG2_OK;
+  int rcd = ensure_descs(s);
+  if (rcd) return rcd;
   const int b = s->cur;
   if (s->graph[b] && (s->graph_dt[b] != dt || s->graph_tend[b] != t_end)) {
     cudaGraphExecDestroy(s->graph[b]);
@@ -594,10 +610,12 @@ int fg2_sim_stage(fg2_sim *s, int k, double dt)
     int rc = do_bcond(s);
     if (rc) return rc;
   }
+  int rc = ensure_descs(s);
+  if (rc) return rc;
   const StageArgs a = stage_args(s, k, dt, nullptr);
   const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
-  const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
-  CK(launch_substage(s->storage, kind, false, m, s->u[1 - s->cur], s->v, s->L, a, s->queue, s->stream));
+  rc = launch_stage(s, kind, false, a, s->desc + s->cur);
+  if (rc) return rc;
   s->cur = 1 - s->cur;
   s->smax_valid = false;
   return FG2_OK;
@@ -641,10 +659,12 @@ int fg2_sim_kick(fg2_sim *s, double t, double beta)
   (void)t;
   if (!s) return fail(FG2_ERR_ARG, "null handle");
   ensure_config(s);
+  int rc = ensure_descs(s);
+  if (rc) return rc;
   StageArgs a = stage_args(s, 0, 0.0, nullptr);
   a.beta = beta;
-  const StageMaps m{&s->map[s->cur], &s->vmap, &s->omap[1 - s->cur], &s->vomap};
-  CK(launch_substage(s->storage, STAGE_KICK, false, m, nullptr, s->v, s->L, a, s->queue, s->stream));
+  rc = launch_stage(s, STAGE_KICK, false, a, s->desc + s->cur);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
   return FG2_OK;
 }
@@ -815,48 +835,23 @@ int fg2_step(double t, double dt) { return g_sim ? fg2_sim_step(g_sim, t, dt) : 
 
 // kick/drift/bcond/Euler take device pointers into arrays of the global layout, as the
 // reference's take interior-origin pointers (src/fg2.h:81-84).
-static int array_index(const void *p)
-{
-  if (!g_sim) return -1;
-  if (p == g_sim->u[0]) return 0;
-  if (p == g_sim->u[1]) return 1;
-  if (p == g_sim->v) return 2;
-  return -1;
-}
-
 void fg2_kick(float *v, const float *u, float t, float beta)
 {
   (void)t;
   if (!g_sim) return;
   ensure_config(g_sim);
-  const int ui = array_index(u);
-  const CUtensorMap *mu = nullptr, *mv = nullptr;
-  if (ui == 0 || ui == 1) mu = &g_sim->map[ui];
-  else {
-    if (g_sim->kick_map_base != u) {
-      if (encode_u_map(&g_sim->kick_map, u, g_sim->L, g_sim->storage) != CUDA_SUCCESS) return;
-      g_sim->kick_map_base = u;
-    }
-    mu = &g_sim->kick_map;
+  // any arrays of the global layout: the descriptor is encoded for these pointers
+  GridDesc &d = g_sim->desc_host[2];
+  if (make_grid_desc(&d, u, nullptr, v, g_sim->L, g_sim->storage, g_sim->p1, g_sim->p2, g_sim->delta1, g_sim->delta2,
+                     nullptr, g_sim->status, 0) != CUDA_SUCCESS) {
+    fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
+    return;
   }
-  const CUtensorMap *mvo = nullptr;
-  if (v == g_sim->v) {
-    mv = &g_sim->vmap;
-    mvo = &g_sim->vomap;
-  } else {
-    if (g_sim->kick_vmap_base != v) {
-      if (encode_v_map(&g_sim->kick_vmap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS ||
-          encode_store_map(&g_sim->kick_vomap, v, g_sim->L, g_sim->storage) != CUDA_SUCCESS)
-        return;
-      g_sim->kick_vmap_base = v;
-    }
-    mv = &g_sim->kick_vmap;
-    mvo = &g_sim->kick_vomap;
-  }
+  if (cudaMemcpyAsync(g_sim->desc + 2, &d, sizeof(GridDesc), cudaMemcpyHostToDevice, g_sim->stream) != cudaSuccess)
+    return;
   StageArgs a = stage_args(g_sim, 0, 0.0, nullptr);
   a.beta = beta;
-  const StageMaps m{mu, mv, mvo, mvo};
-  launch_substage(g_sim->storage, STAGE_KICK, false, m, nullptr, v, g_sim->L, a, g_sim->queue, g_sim->stream);
+  launch_stage(g_sim, STAGE_KICK, false, a, g_sim->desc + 2);
   cudaStreamSynchronize(g_sim->stream);
 }
 

@@ -1,47 +1,59 @@
 // fg2_b200/csrc/substage.cuh -- the fused RK3 substage kernel (included inside namespace fg2
 // by kernels.cu, once per scheme).
 //
-// Work decomposition.  A tile is a strip of SW = 128 interior columns by TH = 35 rows of one
-// simulation.  A persistent grid of CTAs drains a tile queue (an atomic counter that the
-// last CTA to finish resets, so a launch needs no host-side reset and replays from a CUDA
-// graph).  A CTA has 4 warps; a thread owns one column of the strip.
+// Work decomposition.  A launch advances a list of grids (one simulation, or a batch of
+// independent simulations of any sizes).  A tile is a strip of SW = 128 interior columns by
+// TH = 35 rows of one grid; the launch's tiles are numbered grid by grid, strip fastest, and a
+// persistent grid of CTAs drains them from a queue (an atomic counter that the last CTA to
+// finish resets, so a launch needs no host-side reset and replays from a CUDA graph).  A CTA
+// has 4 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in
+// device memory: its TMA tensor maps, output pointers, layout, boundaries, time step and
+// status block.
 //
-// Data movement.  u streams through a ring of NSLOT shared-memory slots by TMA
+// Data movement.  u and v stream through a ring of NSLOT shared-memory slots by TMA
 // (cp.async.bulk.tensor.3d, no multicast): chunk 0 of a tile is the 7-row warm-up box
 // u[i0-4 .. i0+3) x [j0-4, j0+132), chunk b+1 the 7 leading rows u[i0+3+7b ..] of output
-// block b; a box lands as [row][cell][field], the cells' fields interleaved as in HBM, so a
-// thread reads a whole hydro cell with one 16-byte shared load.  When a block's u chunk is
-// issued, the same 7 rows of v are prefetched into L2 (cp.async.bulk.prefetch.tensor), and
-// each thread loads its v values a row before it needs them.  The block's results (u' and
-// the new v) are staged in shared memory and written back with one TMA tensor store per
-// array; the store maps end at the interior's last row and column, so partial tiles clip
-// there and ghost cells are never written by the bulk store (edge cells write their ghost
-// images directly).  One CTA barrier per chunk hands the ring slot and the staging buffer
-// over; every wait on a TMA completion is bounded (%globaltimer) and the CTA agrees on a
-// timeout before leaving, which raises an error bit in the status block.
+// block b together with v of the block's 7 output rows.  A box lands as [row][cell][field],
+// the cells' fields interleaved as in HBM, so a thread reads a whole hydro cell with one
+// 16-byte shared load.  The results u' and v are written by the threads straight from
+// registers (one 16-byte store per cell and array; a warp writes 512 contiguous bytes per row).
+// One CTA barrier per chunk hands the slot back to the producer thread; every wait on a TMA
+// completion is bounded (%globaltimer) and the CTA agrees on a timeout before leaving, which
+// raises an error bit in the launch's status block.
 //
 // Stencil.  Each thread walks its column down the tile.  At every leading row L it loads the
-// 7 cells u(L, j-3..j+3) from shared memory and computes the axis-2
-// (contiguous) derivatives D2 and D22 of row L, pushes u(L, j) into a 7-row register window
-// (the axis-1 stencil of row L-3 then needs no further loads), and feeds the mixed
-// derivative by streaming accumulators: with delta_k(r) = u(r, j+k) - u(r, j-k),
-// D12(r) = sum_k m_k (delta_k(r+k) - delta_k(r-k)), so delta_k(L) is added to row L-k and
-// subtracted from row L+k (src/deriv.h:60-62 regrouped).  Fields are handled in pairs
-// ((lnd, u1), (u2, lne)) so the stencil arithmetic of two fields is one packed FP32x2
-// instruction (add/mul/fma .f32x2 on sm_100).  The output row L-3 then has all its
-// derivatives in registers; the scheme's eqns() gives F, and the epilogue applies
-// v <- F + beta v, u' <- u + gamma dt v (src/kick.cu:53, src/drift.cu:29), stores u' with
-// its ghost images and v, flags NaNs and, on the last stage, folds the CFL rate into a max.
-// Register slots are indexed by row mod 7 and the row loop is unrolled by 7, so the window
-// never moves.
+// 7 cells u(L, j-3..j+3) from shared memory and computes the axis-2 (contiguous) derivatives
+// D2 and D22 of row L, pushes u(L, j) into a 7-row register window (the axis-1 stencil of row
+// L-3 then needs no further loads), and feeds the mixed derivative by streaming accumulators:
+// with delta_k(r) = u(r, j+k) - u(r, j-k), D12(r) = sum_k m_k (delta_k(r+k) - delta_k(r-k)),
+// so delta_k(L) is added to row L-k and subtracted from row L+k (src/deriv.h:60-62
+// regrouped).  Fields are handled in pairs ((lnd, u1), (u2, lne)) so the stencil arithmetic of
+// two fields is one packed FP32x2 instruction (add/mul/fma .f32x2 on sm_100).  The output row
+// L-3 then has all its derivatives in registers; the scheme's eqns() gives F, and the
+// epilogue applies v <- F + beta v, u' <- u + gamma dt v (src/kick.cu:53, src/drift.cu:29),
+// stores u' with its ghost images and v, flags NaNs and, on the last stage, folds the CFL rate
+// into a max.  Register slots are indexed by row mod 7 and the row loop is unrolled by 7, so
+// the window never moves.
+//
+// Stencil weights.  A single-grid launch folds 1/Delta into the weights (constant-bank
+// operands).  A batch launch (SC) uses the reference's plain weights and multiplies each
+// derivative by its grid's 1/Delta factors, which it keeps in registers, as the reference
+// divides by Delta after the weighted sum (src/deriv.h:42-62).
 #pragma once
 
 namespace sub {
 
+#ifndef FG2_NB
+#define FG2_NB 5
+#endif
+#ifndef FG2_NSLOT
+#define FG2_NSLOT 2
+#endif
+
 constexpr int SW = 128;            // interior columns per tile (strip width)
 constexpr int BW = SW + 2 * GL;    // TMA box width of u (halo 4 + 4; the stencil uses 3)
 constexpr int CH = 7;              // rows per chunk = register window period
-constexpr int NB = 5;              // output blocks per tile
+constexpr int NB = FG2_NB;         // output blocks per tile
 constexpr int TH = NB * CH;        // output rows per tile
 constexpr int NCW = 4;             // warps per CTA
 constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
@@ -49,31 +61,26 @@ constexpr int NP = (NV + 1) / 2;   // field pairs
 static_assert(NT == SW, "one thread per strip column");
 static_assert(scheme::U1 == 1 && scheme::U2 == 2, "u1 and u2 are fields 1 and 2");
 
-#ifndef FG2_NSLOT_F32
-#define FG2_NSLOT_F32 2
-#endif
-#ifndef FG2_MIN_CTAS
-#define FG2_MIN_CTAS 1
-#endif
-
-template <class T>
+// Shared memory of one CTA: NSLOT slots of [u box | v box] (the v box only when the stage
+// reads v), then the mbarriers and the producer's bookkeeping.
+template <class T, bool RV>
 struct Geo {
-  static constexpr int NSLOT = sizeof(T) == 8 ? 2 : FG2_NSLOT_F32;
+  static constexpr int NSLOT = FG2_NSLOT;
   static constexpr int G = 16 / (int)sizeof(T);  // cells per 16-byte group (TMA box unit)
   static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * NV * sizeof(T));
-  static constexpr uint32_t SLOT = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
-  static constexpr uint32_t OUT_BYTES = (uint32_t)(SW * CH * NV * sizeof(T));  // one block of one array
-  static constexpr size_t STAGE_OFF = (size_t)NSLOT * SLOT;                     // u' then v staging
-  static constexpr size_t BAR_OFF = STAGE_OFF + 2 * (size_t)OUT_BYTES;
-  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], producer state
-  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + NSLOT * sizeof(int) + 4 * sizeof(int) + 64;
-  static_assert(SLOT % 128 == 0 && OUT_BYTES % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
+  static constexpr uint32_t V_OFF = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
+  static constexpr uint32_t V_BYTES = (uint32_t)(SW * CH * NV * sizeof(T));
+  static constexpr uint32_t SLOT = V_OFF + (RV ? (V_BYTES + 127) / 128 * 128 : 0);
+  static constexpr size_t BAR_OFF = (size_t)NSLOT * SLOT;
+  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
+  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
+  static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
   static_assert(BW % G == 0 && SW % G == 0 && GL % G == 0, "boxes and tile origins are whole cell groups");
   static_assert(BW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
 };
 
 // One cell's NV values as field pairs ((lnd, u1), (u2, lne)): one or two 16-byte accesses for
-// a hydro cell, scalar ones for a 3-field cell.  The _cs forms stream through the caches.
+// a hydro cell, scalar ones for a 3-field cell.
 template <class T>
 __device__ __forceinline__ void ld_cell(const T *p, typename PairOf<T>::type out[NP])
 {
@@ -88,23 +95,6 @@ __device__ __forceinline__ void ld_cell(const T *p, typename PairOf<T>::type out
   } else {
 #pragma unroll
     for (int q = 0; q < NP; ++q) out[q] = PO::make(p[2 * q], 2 * q + 1 < NV ? p[2 * q + 1] : T(0));
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void ld_cell_cs(const T *p, typename PairOf<T>::type out[NP])
-{
-  using PO = PairOf<T>;
-  if constexpr (NV == 4 && sizeof(T) == 4) {
-    const float4 x = __ldcs(reinterpret_cast<const float4 *>(p));
-    out[0] = make_float2(x.x, x.y);
-    out[1] = make_float2(x.z, x.w);
-  } else if constexpr (NV == 4 && sizeof(T) == 8) {
-    out[0] = __ldcs(reinterpret_cast<const double2 *>(p));
-    out[1] = __ldcs(reinterpret_cast<const double2 *>(p + 2));
-  } else {
-#pragma unroll
-    for (int q = 0; q < NP; ++q) out[q] = PO::make(__ldcs(p + 2 * q), 2 * q + 1 < NV ? __ldcs(p + 2 * q + 1) : T(0));
   }
 }
 
@@ -125,8 +115,8 @@ __device__ __forceinline__ void st_cell(T *p, const typename PairOf<T>::type in[
   }
 }
 
-// Tile t of a single grid: strip fastest, so horizontally adjacent tiles run together and
-// share their halo columns through L2.
+// Tiles of one grid: strip fastest, so horizontally adjacent tiles run together and share
+// their halo columns through L2.
 struct TileGrid {
   int strips, rows, ntiles;
 };
@@ -157,12 +147,18 @@ struct Roll {
   T x[2][CH];     // D12 accumulators of u1, u2
 };
 
-__device__ __forceinline__ bool bounded_wait(uint64_t *bar, uint32_t parity, Status *st)
-{
-  if (mbar_wait_bounded(bar, parity, WAIT_NS)) return true;
-  atomicOr(&st->error, ERR_TMA_TIMEOUT);
-  return false;
-}
+// Everything a thread needs of the grid its current tile belongs to (registers).
+template <class T>
+struct GridRegs {
+  using P = typename PairOf<T>::type;
+  Layout L;
+  T *u_out, *v;
+  Status *status;
+  int p1, p2;
+  P gdt;                       // gamma dt of this grid's step, both lanes
+  P s1, s2, s11, s22;          // 1/Delta factors (batch launches)
+  T s12, inv1, inv2, delta1;   // 1/(Delta1 Delta2), CFL factors, Delta1
+};
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
@@ -224,32 +220,18 @@ __device__ __forceinline__ void lead_row(const T *su, int tx, const KParams<T> &
   }
 }
 
-// v of output row i (pairs of fields), loaded a row before use; `ok` false skips the load.
-template <class T, bool READ_V>
-__device__ __forceinline__ void load_v(const T *v, const Layout &L, int i, int j, bool ok,
-                                       typename PairOf<T>::type vr[NP])
-{
-  using P = typename PairOf<T>::type;
-  if (!READ_V) return;
-  if (ok && i < L.n1 && j < L.n2) {
-    ld_cell_cs<T>(v + L.at(0, i, j), vr);
-  } else {
-#pragma unroll
-    for (int p = 0; p < NP; ++p) vr[p] = lit<P>(0.0);
-  }
-}
-
 // Derivatives of field pair PI at the output row held in register slot S0, into a Cell.
-template <class T, unsigned M2, int S0, int PI>
-__device__ __forceinline__ void emit_pair(const KParams<T> &a, const Roll<T> &s, Cell<T, NV> &cell)
+template <class T, unsigned M2, bool SC, int S0, int PI>
+__device__ __forceinline__ void emit_pair(const KParams<T> &a, const GridRegs<T> &gr, const Roll<T> &s,
+                                          Cell<T, NV> &cell)
 {
   using P = typename PairOf<T>::type;
   const P c = s.w[PI][S0];
   const P p1 = s.w[PI][(S0 + 1) % CH], n1 = s.w[PI][(S0 + 6) % CH];
   const P p2 = s.w[PI][(S0 + 2) % CH], n2 = s.w[PI][(S0 + 5) % CH];
   const P p3 = s.w[PI][(S0 + 3) % CH], n3 = s.w[PI][(S0 + 4) % CH];
-  const P d1 = fmac(a.k.a1[0], p1 - n1, fmac(a.k.a1[1], p2 - n2, a.k.a1[2] * (p3 - n3)));
-  const P d2 = s.h2[PI][S0];
+  P d1 = fmac(a.k.a1[0], p1 - n1, fmac(a.k.a1[1], p2 - n2, a.k.a1[2] * (p3 - n3)));
+  P d2 = s.h2[PI][S0];
   constexpr bool nx = need<M2>(2 * PI), ny = need<M2>(2 * PI + 1);
   P d11 = lit<P>(0.0), d22 = lit<P>(0.0);
   if constexpr (nx && ny) {
@@ -261,6 +243,14 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const Roll<T> &s,
   } else if constexpr (ny) {
     d11.y = fmac(a.ks.b1[0], c.y, fmac(a.ks.b1[1], p1.y + n1.y, fmac(a.ks.b1[2], p2.y + n2.y, a.ks.b1[3] * (p3.y + n3.y))));
     d22.y = s.h22[PI][S0].y;
+  }
+  if constexpr (SC) {
+    d1 = d1 * gr.s1;
+    d2 = d2 * gr.s2;
+    if constexpr (nx || ny) {
+      d11 = d11 * gr.s11;
+      d22 = d22 * gr.s22;
+    }
   }
   cell.q[2 * PI] = c.x;
   cell.d1[2 * PI] = d1.x;
@@ -277,139 +267,193 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const Roll<T> &s,
 }
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
-// Results go to the block's staging buffers (rows [R][cell][field]); edge cells also write
-// their ghost images to u_out.
-template <class T, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
-__device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], int i, int j, int tx,
-                                         const KParams<T> &a, typename PairOf<T>::type gdt2, const Layout &L,
-                                         T *stage_u, T *stage_v, T *u_out, T *v, const Roll<T> &s, bool &nan, T &rate)
+// vr is v of the cell (read stages).  u' and v go straight to HBM; edge cells also write
+// their ghost images.
+template <class T, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
+__device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], int i, int j, const KParams<T> &a,
+                                         const GridRegs<T> &gr, const Roll<T> &s, bool &nan, T &rate)
 {
   using P = typename PairOf<T>::type;
   constexpr int S0 = (R + 4) % CH;
   Cell<T, NV> cell;
-  emit_pair<T, M2, S0, 0>(a, s, cell);
-  if constexpr (NP > 1) emit_pair<T, M2, S0, 1>(a, s, cell);
+  emit_pair<T, M2, SC, S0, 0>(a, gr, s, cell);
+  if constexpr (NP > 1) emit_pair<T, M2, SC, S0, 1>(a, gr, s, cell);
 #pragma unroll
   for (int f = 0; f < NV; ++f) cell.d12[f] = T(0);
-  cell.d12[scheme::U1] = s.x[0][S0];
-  cell.d12[scheme::U2] = s.x[1][S0];
+  cell.d12[scheme::U1] = SC ? s.x[0][S0] * gr.s12 : s.x[0][S0];
+  cell.d12[scheme::U2] = SC ? s.x[1][S0] * gr.s12 : s.x[1][S0];
 
   T r[NV];
-  scheme::eqns<M2>(cell, a.p, i, j, r, a.ks.delta1);
+  scheme::eqns<M2>(cell, a.p, i, j, r, SC ? gr.delta1 : a.ks.delta1);
+  if (i >= gr.L.n1 || j >= gr.L.n2) return;  // cells past the grid
   P vn[NP], qp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     vn[p] = PairOf<T>::make(r[2 * p], 2 * p + 1 < NV ? r[2 * p + 1] : T(0));
     if (READ_V) vn[p] = fmac(a.beta2, vr[p], vn[p]);
-    qp[p] = fmac(gdt2, vn[p], s.w[p][S0]);
+    qp[p] = fmac(gr.gdt, vn[p], s.w[p][S0]);
   }
-  const int so = (R * SW + tx) * NV;
-  if (WRITE_V) st_cell<T>(stage_v + so, vn);
-  if (WRITE_U) st_cell<T>(stage_u + so, qp);
-  if (i >= L.n1 || j >= L.n2) return;  // cells past the grid: staged values are clipped by the store
-  T qn[NV];
+  const long long o = gr.L.at(0, i, j);
+  if (WRITE_U) st_cell<T>(gr.u_out + o, qp);
+  if (WRITE_V) st_cell<T>(gr.v + o, vn);
+  if (WRITE_U) {
+    T qn[NV];
 #pragma unroll
-  for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
+    for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
 #pragma unroll
-  for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
-  if (j >= a.store_cols) {  // interior columns past the bulk stores' last whole cell group
-    const long long o = L.at(0, i, j);
-    if (WRITE_U) st_cell<T>(u_out + o, qp);
-    if (WRITE_V) st_cell<T>(v + o, vn);
+    for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
+    store_ghosts<T, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
+    if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2));
   }
-  if (WRITE_U) store_ghosts<T, T>(u_out, L, i, j, qn, a.p1, a.p2);
-  if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, a.ks));
 }
 
 // Shared state of the chunk issue, read and written by thread 0 only.
 struct Producer {
   int next_n;  // index of the next chunk to issue
-  int tile;    // tile of that chunk
+  int tile;    // launch tile of that chunk
+  int g;       // its grid
+  int i0, j0;  // its origin in the grid
   int c;       // chunk index within the tile (0 = warm-up)
   int done;    // the end-of-queue sentinel was issued
 };
 
+// Grid of launch tile t: the last grid whose first tile is <= t (grids are in tile order).
+__device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, int t)
+{
+  int lo = 0, hi = ngrids - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (grids[mid].tile0 <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Issues the next chunk of the CTA's sequence into its slot (free by the caller's check).
 template <class T, bool READ_V>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
-                                            const CUtensorMap *tm_u, const CUtensorMap *tm_v, int *queue,
-                                            const TileGrid &tg)
+                                            int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int *queue)
 {
-  using G = Geo<T>;
+  using G = Geo<T, READ_V>;
   if (ps->done) return;
   const int n = ps->next_n, s = n % G::NSLOT;
   if (ps->c == 0) {
     int t = atomicAdd(&queue[0], 1);
-    if (t >= tg.ntiles) t = -1;
+    if (t >= ntiles) t = -1;
     ps->tile = t;
     tile_of[s] = t;
+    if (t >= 0) {
+      const int g = grid_of_tile(grids, ngrids, t);
+      const int local = t - grids[g].tile0, strips = grids[g].strips;
+      ps->g = g;
+      ps->i0 = (local / strips) * TH;
+      ps->j0 = (local % strips) * SW;
+      grid_of[s] = g;
+    }
   }
   if (ps->tile < 0) {
     mbar_arrive(&full[s]);
     ps->done = 1;
   } else {
-    const int i0 = (ps->tile / tg.strips) * TH, j0 = (ps->tile % tg.strips) * SW;
-    const int c = ps->c;
-    mbar_arrive_expect_tx(&full[s], G::U_BYTES);
+    const GridDesc &gd = grids[ps->g];
+    const int i0 = ps->i0, j0 = ps->j0, c = ps->c;
+    const bool with_v = READ_V && c > 0;
+    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u));
     // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
     // columns j0 - 4 .. (padded column j0)
-    tma_load_3d(smem + (size_t)s * G::SLOT, tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
-    // the v rows this chunk's output block updates, into L2 ahead of the threads' loads
-    if (READ_V && c > 0) tma_prefetch_l2_3d(tm_v, 0, (j0 + GL) / G::G, i0 + CH * (c - 1) + GT);
+    tma_load_3d(smem + (size_t)s * G::SLOT, &gd.tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
+    // v of the 7 output rows of block c - 1
+    if (with_v)
+      tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL) / G::G,
+                  i0 + CH * (c - 1) + GT);
     ps->c = c == NB ? 0 : c + 1;
   }
   ps->next_n = n + 1;
 }
 
-template <class T, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL>
-__global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid_constant__ CUtensorMap tm_u,
-                                                                    const __grid_constant__ CUtensorMap tm_v,
-                                                                    const __grid_constant__ CUtensorMap tm_uo,
-                                                                    const __grid_constant__ CUtensorMap tm_vo,
-                                                                    T *__restrict__ u_out, T *__restrict__ v,
-                                                                    const Layout L, const KParams<T> a, int *queue)
+// Loads the registers of grid g (every thread; the loads are uniform across the CTA).
+template <class T, bool SC>
+__device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<T> &a, GridRegs<T> &gr)
 {
   using P = typename PairOf<T>::type;
-  using G = Geo<T>;
+  gr.L = gd.L;
+  gr.u_out = reinterpret_cast<T *>(gd.u_out);
+  gr.v = reinterpret_cast<T *>(gd.v);
+  gr.status = gd.status;
+  gr.p1 = gd.p1;
+  gr.p2 = gd.p2;
+  // (R)(dt * gamma[i]), src/step.cpp:34
+  gr.gdt = lit<P>(a.gamma * (gd.dt ? *gd.dt : a.dt_dev ? *a.dt_dev : a.dt));
+  if (SC) {
+    gr.s1 = lit<P>(gd.inv1);
+    gr.s2 = lit<P>(gd.inv2);
+    gr.s11 = lit<P>(gd.inv11);
+    gr.s22 = lit<P>(gd.inv22);
+    gr.s12 = (T)gd.inv12;
+    gr.inv1 = (T)gd.inv1;
+    gr.inv2 = (T)gd.inv2;
+    gr.delta1 = (T)gd.delta1;
+  } else {
+    gr.inv1 = a.ks.inv1;
+    gr.inv2 = a.ks.inv2;
+  }
+}
+
+// Publishes a grid's NaN flag and CFL max (CTA-uniform call; warp-level reductions).
+template <bool WRITE_U, bool CFL, class T>
+__device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
+{
+  const int lane = threadIdx.x & 31;
+  if (WRITE_U) {
+    if (__any_sync(0xffffffffu, nan) && lane == 0) atomicOr(&st->nan, 1u);
+  }
+  if (CFL) {
+    double r = (double)rate;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+    if (lane == 0 && r > 0.0) atomicMax(&st->smax, (unsigned long long)__double_as_longlong(r));
+  }
+  nan = false;
+  rate = T(0);
+}
+
+template <class T, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
+__global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
+                                                         const KParams<T> a, int *queue)
+{
+  using P = typename PairOf<T>::type;
+  using G = Geo<T, READ_V>;
   constexpr int NS = G::NSLOT;
   extern __shared__ __align__(128) unsigned char smem[];
-  T *stage_u = reinterpret_cast<T *>(smem + G::STAGE_OFF);
-  T *stage_v = reinterpret_cast<T *>(smem + G::STAGE_OFF + G::OUT_BYTES);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
   int *tile_of = reinterpret_cast<int *>(full + NS);
-  Producer *ps = reinterpret_cast<Producer *>(tile_of + NS);
-  const TileGrid tg = tile_grid(L);
-  const int lane = threadIdx.x & 31;
+  int *grid_of = tile_of + NS;
+  Producer *ps = reinterpret_cast<Producer *>(grid_of + NS);
 
   if (threadIdx.x == 0) {
-    prefetch_tmap(&tm_u);
-    if (READ_V) prefetch_tmap(&tm_v);
-    if (WRITE_U) prefetch_tmap(&tm_uo);
-    if (WRITE_V) prefetch_tmap(&tm_vo);
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
     ps->next_n = 0;
     ps->tile = -1;
+    ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<T, READ_V>(ps, smem, full, tile_of, &tm_u, &tm_v, queue, tg);
+    for (int s = 0; s < NS; ++s) issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, queue);
   }
   __syncthreads();
 
   bool nan = false;
   T rate = T(0);
   const int tx = threadIdx.x;  // column within the strip
-  const P gdt2 = lit<P>(a.gamma * (a.dt_dev ? *a.dt_dev : a.dt));  // (R)(dt * gamma[i]), src/step.cpp:34
+  GridRegs<T> gr;
+  int cur_g = -1;
   Roll<T> st;
   int n = 0;  // chunks consumed
   int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
-  P vr[2][NP];
 
   for (;;) {
     const int s = n % NS;
-    // the chunk has landed (every thread waits, the CTA agrees) and, for thread 0's last
-    // bulk stores, the staging buffers have been read out
-    if (threadIdx.x == 0 && (WRITE_U || WRITE_V)) bulk_wait_read_all();
+    // the chunk has landed (every thread waits, the CTA agrees)
     const bool landed = mbar_wait_bounded(&full[s], (uint32_t)((n / NS) & 1), WAIT_NS);
     if (__syncthreads_or(!landed)) {
       if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
@@ -419,13 +463,19 @@ __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid
     if (b < 0) {
       const int tile = tile_of[s];
       if (tile < 0) break;
-      i0 = (tile / tg.strips) * TH;
-      j0 = (tile % tg.strips) * SW;
+      const int g = grid_of[s];
+      if (g != cur_g) {
+        if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);
+        load_grid<T, SC>(grids[g], a, gr);
+        cur_g = g;
+      }
+      const int local = tile - grids[g].tile0, strips = grids[g].strips;
+      i0 = (local / strips) * TH;
+      j0 = (local % strips) * SW;
 #pragma unroll
-      for (int g = 0; g < 2; ++g)
+      for (int g2 = 0; g2 < 2; ++g2)
 #pragma unroll
-        for (int q = 0; q < CH; ++q) st.x[g][q] = T(0);
-      load_v<T, READ_V>(v, L, i0, j0 + tx, true, vr[0]);  // v of the tile's first output row
+        for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
       // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
       lead_row<T, M2, 0>(su, tx, a, st);
       lead_row<T, M2, 1>(su, tx, a, st);
@@ -436,47 +486,28 @@ __global__ void __launch_bounds__(NT, FG2_MIN_CTAS) substage_kernel(const __grid
       lead_row<T, M2, 6>(su, tx, a, st);
     } else {
       const int ib = i0 + CH * b, j = j0 + tx;
-      // row R uses vr[R & 1] and loads the next row into vr[(R + 1) & 1]; a block has an odd
-      // number of rows, so it ends by moving the loaded row to vr[0]
-#define FG2_ROW(R)                                                                                        \
-  load_v<T, READ_V>(v, L, ib + R + 1, j, CH * b + R + 1 < TH, vr[(R + 1) & 1]);                           \
-  lead_row<T, M2, R>(su, tx, a, st);                                                                      \
-  emit_row<T, M2, R, READ_V, WRITE_V, WRITE_U, CFL>(vr[R & 1], ib + R, j, tx, a, gdt2, L, stage_u, stage_v, \
-                                                    u_out, v, st, nan, rate);
+      const T *sv = su + G::V_OFF / sizeof(T);
+#define FG2_ROW(R)                                                                                \
+  {                                                                                               \
+    P vrow[NP];                                                                                   \
+    if (READ_V) ld_cell<T>(sv + (R * SW + tx) * NV, vrow);                                        \
+    lead_row<T, M2, R>(su, tx, a, st);                                                            \
+    emit_row<T, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
+  }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
-#pragma unroll
-      for (int p = 0; p < NP; ++p) vr[0][p] = vr[1][p];
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // staged results -> bulk stores
     }
-    __syncthreads();  // everyone is done with slot s and has staged its results
-    if (threadIdx.x == 0) {
-      if (b >= 0 && i0 + CH * b < L.n1) {
-        // interior rows ib .. ib+6 of the strip; the maps clip at the last interior row/column
-        const int ib = i0 + CH * b;
-        if (WRITE_U) tma_store_3d(&tm_uo, stage_u, 0, (j0 + GL) / G::G, ib + GT);
-        if (WRITE_V) tma_store_3d(&tm_vo, stage_v, 0, (j0 + GL) / G::G, ib + GT);
-        if (WRITE_U || WRITE_V) bulk_commit();
-      }
-      issue_chunk<T, READ_V>(ps, smem, full, tile_of, &tm_u, &tm_v, queue, tg);  // refill slot s
-    }
+    __syncthreads();  // everyone is done with slot s
+    if (threadIdx.x == 0)
+      issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, queue);  // refill slot s
     ++n;
     b = b == NB - 1 ? -1 : b + 1;
   }
 
-  if (WRITE_U) {
-    if (__any_sync(0xffffffffu, nan) && lane == 0) atomicOr(&a.status->nan, 1u);
-  }
-  if (CFL) {
-    double r = (double)rate;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
-    if (lane == 0 && r > 0.0) atomicMax(&a.status->smax, (unsigned long long)__double_as_longlong(r));
-  }
+  if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);
 
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (WRITE_U || WRITE_V) bulk_wait_all();  // the bulk stores have completed
     // after an error, let every load this CTA issued land before the CTA exits
     const int issued = ps->next_n;
     for (int s = 0; s < NS && s < issued; ++s) {
