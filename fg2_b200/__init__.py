@@ -66,6 +66,15 @@ def _bind(lib):
         "fg2_drift": (None, [P, P, ctypes.c_float]), "fg2_bcond": (None, [P, I, I]),
         "fg2_Euler": (None, [P, ctypes.c_float]), "fg2_global": (P, []),
         "fg2_sums_noalloc": (I, [P, I, I, LL, I, P, P]),
+        "fg2_batch_create": (P, [I, P, P, I, P]), "fg2_batch_destroy": (None, [P]),
+        "fg2_batch_count": (I, [P]), "fg2_batch_cells": (LL, [P]), "fg2_batch_device_bytes": (SZ, [P]),
+        "fg2_batch_stream": (P, [P]), "fg2_batch_member": (P, [P, I]),
+        "fg2_batch_set_box": (I, [P, D, D]), "fg2_batch_set_courant": (I, [P, D]),
+        "fg2_batch_set_bcond": (I, [P, I, I]), "fg2_batch_para": (S, [P, S]), "fg2_batch_config": (I, [P]),
+        "fg2_batch_set_time": (I, [P, D]), "fg2_batch_advance": (I, [P, I, D, D, I]),
+        "fg2_batch_sync": (I, [P]), "fg2_batch_set_tiling": (I, [P, I, I]),
+        "fg2_batch_get_tiling": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "fg2_batch_autotune": (I, [P, I, ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -107,21 +116,23 @@ def setup_evaluate(name, n1, n2, scheme="hydro", l1=1.0, l2=1.0, para=None, seed
 class Sim:
     """One simulation on the current CUDA device (the handle API, fg2_sim_*)."""
 
-    def __init__(self, n1, n2, scheme="hydro", storage="f32", stream=None):
+    def __init__(self, n1, n2, scheme="hydro", storage="f32", stream=None, _member=None):
         self.lib = load_library(scheme)
         self.scheme = self.lib.fg2_scheme_name().decode()
         self.n1, self.n2 = int(n1), int(n2)
         self.storage = storage
         self.nvar = self.lib.fg2_nvar()
         self.host_dtype = np.float64 if storage == "f64" else np.float32
-        h = self.lib.fg2_sim_create(self.n1, self.n2, STORAGE[storage], stream)
+        self._owner = _member is None
+        h = self.lib.fg2_sim_create(self.n1, self.n2, STORAGE[storage], stream) if self._owner else _member
         if not h:
             raise FG2Error(self.lib.fg2_last_error().decode())
         self.h = ctypes.c_void_p(h)
 
     def close(self):
         if getattr(self, "h", None):
-            self.lib.fg2_sim_destroy(self.h)
+            if self._owner:
+                self.lib.fg2_sim_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -269,3 +280,104 @@ class Sim:
         t = ctypes.c_double()
         self._check(self.lib.fg2_sim_load(self.h, str(path).encode(), ctypes.byref(t)), "load")
         return t.value
+
+
+class Batch:
+    """Independent simulations of one scheme advanced together (the batch API, fg2_batch_*).
+
+    `sizes` is a list of (n1, n2).  `members[k]` is a Sim view of member k (owned by the batch)
+    for init, upload/download, sums, time and per-member status."""
+
+    def __init__(self, sizes, scheme="hydro-isot", storage="f32", stream=None):
+        self.lib = load_library(scheme)
+        sizes = [(int(a), int(b)) for a, b in sizes]
+        n = len(sizes)
+        n1 = (ctypes.c_int * n)(*[a for a, _ in sizes])
+        n2 = (ctypes.c_int * n)(*[b for _, b in sizes])
+        h = self.lib.fg2_batch_create(n, ctypes.cast(n1, ctypes.c_void_p), ctypes.cast(n2, ctypes.c_void_p),
+                                      STORAGE[storage], stream)
+        if not h:
+            raise FG2Error(self.lib.fg2_last_error().decode())
+        self.h = ctypes.c_void_p(h)
+        self.sizes = sizes
+        self.members = [Sim(a, b, scheme, storage, _member=self.lib.fg2_batch_member(self.h, k))
+                        for k, (a, b) in enumerate(sizes)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None
+            self.lib.fg2_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc < 0 or rc > 1:
+            raise FG2Error(f"{what}: status {rc}: {self.lib.fg2_last_error().decode()}")
+        return rc
+
+    def __len__(self):
+        return len(self.members)
+
+    @property
+    def cells(self):
+        return self.lib.fg2_batch_cells(self.h)
+
+    @property
+    def device_bytes(self):
+        return self.lib.fg2_batch_device_bytes(self.h)
+
+    @property
+    def stream(self):
+        return self.lib.fg2_batch_stream(self.h)
+
+    def para(self, keyval):
+        r = self.lib.fg2_batch_para(self.h, keyval.encode())
+        return None if r is None else r.decode()
+
+    def set_box(self, l1, l2):
+        self._check(self.lib.fg2_batch_set_box(self.h, l1, l2), "set_box")
+
+    def set_courant(self, c):
+        self._check(self.lib.fg2_batch_set_courant(self.h, c), "set_courant")
+
+    def set_bcond(self, p1, p2):
+        self._check(self.lib.fg2_batch_set_bcond(self.h, int(p1), int(p2)), "set_bcond")
+
+    def config(self):
+        self._check(self.lib.fg2_batch_config(self.h), "config")
+
+    def set_time(self, t):
+        self._check(self.lib.fg2_batch_set_time(self.h, float(t)), "set_time")
+
+    def advance(self, nsteps, dt=0.0, t_end=float("inf"), graph=True):
+        """nsteps RK3 steps of every member (dt <= 0: per-member device-resident CFL steps)."""
+        return self._check(self.lib.fg2_batch_advance(self.h, int(nsteps), float(dt), float(t_end), int(bool(graph))),
+                           "advance")
+
+    def sync(self):
+        return self.lib.fg2_batch_sync(self.h)
+
+    def set_tiling(self, nb, ctas_per_sm=0):
+        self._check(self.lib.fg2_batch_set_tiling(self.h, int(nb), int(ctas_per_sm)), "set_tiling")
+
+    def tiling(self):
+        nb, c = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.fg2_batch_get_tiling(self.h, ctypes.byref(nb), ctypes.byref(c)), "tiling")
+        return nb.value, c.value
+
+    def autotune(self, reps=3):
+        ms = ctypes.c_double()
+        self._check(self.lib.fg2_batch_autotune(self.h, int(reps), ctypes.byref(ms)), "autotune")
+        return ms.value

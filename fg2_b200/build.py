@@ -21,7 +21,7 @@ SCHEMES = ("hydro", "hydro-isot")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"] + ARCH
-SOURCES = ("kernels.cu", "noalloc.cu", "runtime.cpp")
+SOURCES = ("kernels.cu", "noalloc.cu", "runtime.cpp", "batch.cpp")
 
 
 def nvcc():

@@ -2,8 +2,8 @@
 // scheme (-I schemes/<name>), for sm_100a.
 //
 // The hot kernel is the fused RK3 substage (substage_kernel): one pass per stage that
-//   1. stages a (TH + 6) x (TW + 8) x NVAR tile of u, halo included, from HBM into shared
-//      memory with one TMA box load (cp.async.bulk.tensor.3d, completion on an mbarrier);
+//   1. streams 7-row chunks of u (halo included) and v of a 128-column strip from HBM into
+//      shared memory by TMA (cp.async.bulk.tensor.3d, completion on an mbarrier);
 //   2. evaluates the 6th-order derivatives and the scheme's right-hand side per cell
 //      (src/kick.cu:59-106 + src/deriv.h:39-63 + <scheme>/eqns.cuh);
 //   3. applies the low-storage RK3 register update in the epilogue,
@@ -60,6 +60,7 @@ struct KParams {
   double gamma, dt;
   const double *dt_dev;  // device time step for grids without their own, or null: dt
   Status *status;        // launch errors
+  int nb;                // output blocks of 7 rows per tile
 };
 
 template <class T>
@@ -113,6 +114,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.dt = a.dt;
   kp.dt_dev = a.dt_dev;
   kp.status = a.status;
+  kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
   return kp;
 }
 
@@ -242,7 +244,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   d->u_out = u_out;
   d->v = v;
   d->L = L;
-  d->strips = sub::tile_grid(L).strips;
+  d->strips = sub::tile_grid(L, sub::NB_DEFAULT).strips;
   d->tile0 = tile0;
   d->p1 = p1;
   d->p2 = p2;
@@ -257,11 +259,11 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   return CUDA_SUCCESS;
 }
 
-int substage_tiles(const Layout &L) { return sub::tile_grid(L).ntiles; }
+int substage_tiles(const Layout &L, int nb) { return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT).ntiles; }
 
 template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
-static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<T> &kp, int *queue,
-                                cudaStream_t s)
+static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<T> &kp, int max_ctas,
+                                int *queue, cudaStream_t s)
 {
   using G = sub::Geo<T, RV>;
   auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF, SC>;
@@ -277,23 +279,23 @@ static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, c
     if (ctas_per_sm < 1) return cudaErrorInvalidConfiguration;
   }
   if (ntiles < 1) return cudaSuccess;
-  int grid = sms * ctas_per_sm;
+  int grid = sms * (max_ctas > 0 && max_ctas < ctas_per_sm ? max_ctas : ctas_per_sm);
   if (grid > ntiles) grid = ntiles;
   kern<<<grid, sub::NT, G::SMEM, s>>>(grids, ngrids, ntiles, kp, queue);
   return cudaGetLastError();
 }
 
 template <class T, unsigned M2, bool SC>
-static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int nt, const KParams<T> &kp, int *queue,
-                              cudaStream_t s)
+static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int nt, const KParams<T> &kp, int mc,
+                              int *queue, cudaStream_t s)
 {
   switch (kind) {
-    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false, SC>(g, ng, nt, kp, queue, s);
-    case STAGE_MID: return run_substage<T, M2, true, true, true, false, SC>(g, ng, nt, kp, queue, s);
+    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
+    case STAGE_MID: return run_substage<T, M2, true, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
     case STAGE_LAST:
-      return cfl ? run_substage<T, M2, true, false, true, true, SC>(g, ng, nt, kp, queue, s)
-                 : run_substage<T, M2, true, false, true, false, SC>(g, ng, nt, kp, queue, s);
-    case STAGE_KICK: return run_substage<T, M2, true, true, false, false, SC>(g, ng, nt, kp, queue, s);
+      return cfl ? run_substage<T, M2, true, false, true, true, SC>(g, ng, nt, kp, mc, queue, s)
+                 : run_substage<T, M2, true, false, true, false, SC>(g, ng, nt, kp, mc, queue, s);
+    case STAGE_KICK: return run_substage<T, M2, true, true, false, false, SC>(g, ng, nt, kp, mc, queue, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -308,9 +310,9 @@ static cudaError_t substage_t(int kind, bool cfl, const GridDesc *g, int ng, int
   const KParams<T> kp = make_params<T>(a, SC);
   const unsigned need = scheme::d2_fields(a.para);
   if constexpr (sizeof(T) == 4) {
-    if ((need & ~scheme::D2_DEFAULT) == 0) return substage_m<T, scheme::D2_DEFAULT, SC>(kind, cfl, g, ng, nt, kp, queue, s);
+    if ((need & ~scheme::D2_DEFAULT) == 0) return substage_m<T, scheme::D2_DEFAULT, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
   }
-  return substage_m<T, scheme::D2_ALL, SC>(kind, cfl, g, ng, nt, kp, queue, s);
+  return substage_m<T, scheme::D2_ALL, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
 }
 
 cudaError_t launch_substage(int storage, int kind, bool cfl, bool scaled, const GridDesc *grids, int ngrids,
@@ -486,6 +488,26 @@ __global__ void dt_update_kernel(Status *st, double courant, double dt_diff, dou
   st->steps += 1ull;
 }
 
+// Device-resident time steps of a batch: member k takes min(courant_k / smax_k, dt_diff_k),
+// capped at t_end, exactly as dt_update_kernel does for one simulation.
+__global__ void dt_update_batch_kernel(Status *st, const double2 *limits, int count, double t_end)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  Status &s = st[k];
+  const double courant = limits[k].x, dt_diff = limits[k].y;
+  const double smax = __longlong_as_double((long long)s.smax);
+  double dt = smax > 0.0 ? courant / smax : dt_diff;
+  if (dt_diff > 0.0 && dt_diff < dt) dt = dt_diff;
+  const double left = t_end - s.t;
+  if (left < dt) dt = left > 0.0 ? left : 0.0;
+  s.dt = dt;
+  s.dt_next = dt;
+  s.t += dt;
+  s.smax = 0ull;
+  s.steps += 1ull;
+}
+
 // ---------------------------------------------------------------------------------------
 // launchers
 static int grid_for(long long n, int threads)
@@ -564,6 +586,13 @@ cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *par
   else if (storage == ST_F64) sums_kernel<double><<<nb, SUM_THREADS, 0, s>>>((const double *)u, L, partials);
   else return cudaErrorInvalidValue;
   sums_final_kernel<<<1, SUM_THREADS, 0, s>>>(partials, nb, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt_update_batch(Status *st, const double2 *limits, int count, double t_end, cudaStream_t s)
+{
+  if (count < 1) return cudaSuccess;
+  dt_update_batch_kernel<<<(count + 127) / 128, 128, 0, s>>>(st, limits, count, t_end);
   return cudaGetLastError();
 }
 

@@ -24,6 +24,8 @@ struct StageArgs {
   const double *para;   // scheme parameters by slot
   int p1, p2;           // boundary kind per axis (BC_PERIODIC / BC_WALL)
   Status *status;       // device status block (launch errors; per-grid blocks are in GridDesc)
+  int nb = 0;           // tile height in blocks of 7 rows (0: the default)
+  int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
 };
 
 enum StageKind : int {
@@ -56,7 +58,10 @@ struct GridDesc {
 // driver's error.
 CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
                         int p2, double delta1, double delta2, const double *dt, Status *status, int tile0);
-int substage_tiles(const Layout &L);
+// Tile height of the substage kernel in blocks of 7 output rows, unless a launch sets nb.
+constexpr int TILE_BLOCKS_DEFAULT = 5;
+// Tiles of one grid for a tile height of nb blocks of 7 rows (0: the default).
+int substage_tiles(const Layout &L, int nb = 0);
 
 // One fused substage over the grids of `grids` (device array of ngrids descriptors holding
 // ntiles tiles in all).  `scaled`: the grids differ in Delta (stencil weights scaled per grid);
@@ -83,5 +88,7 @@ cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *par
 // (applied by the caller's order: the update runs before the step that uses dt and
 // advances t by it), smax reset to 0 for the step's last stage to refill.
 cudaError_t launch_dt_update(Status *status, double courant, double dt_diff, double t_end, cudaStream_t s);
+// The same for the count members of a batch (status[k]; limits[k] = {courant, dt_diff}).
+cudaError_t launch_dt_update_batch(Status *status, const double2 *limits, int count, double t_end, cudaStream_t s);
 
 }  // namespace fg2

@@ -18,10 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/fg2_b200.h"
-#include "fg2b.h"
-#include "kernels.h"
-#include "setup_common.h"
+#include "sim.h"
 
 #include <state.h>
 #include <eqns.cuh>
@@ -44,9 +41,8 @@ int fg2::set_error(int code, const char *fmt, ...)
   return code;
 }
 
-namespace {
-
-#define fail fg2::set_error
+namespace fg2 {
+namespace rt {
 
 int cuda_status(cudaError_t e, const char *what)
 {
@@ -54,60 +50,19 @@ int cuda_status(cudaError_t e, const char *what)
   return fail((int)e, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CK(expr)                                          \
-  do {                                                    \
-    cudaError_t e_ = (expr);                              \
-    if (e_ != cudaSuccess) return cuda_status(e_, #expr); \
-  } while (0)
-
 size_t elem_size(int storage) { return storage == ST_F64 ? 8 : storage == ST_F32 ? 4 : 2; }
 size_t host_elem(int storage) { return storage == ST_F64 ? 8 : 4; }
 
-// RK3 coefficients (src/step.cpp:24-26), evaluated in double as the reference's E.
 const double RK_ALPHA[3] = {0.0, 1.0 / 3.0, 3.0 / 4.0};
 const double RK_BETA[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
 const double RK_GAMMA[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
 
+namespace {
 // 6th-order second-derivative symbol maximum (1088/180 per axis) and the RK3 real-axis
 // stability bound: the explicit diffusive limit is dt <= c_d * 2.51 / (D (6.04/D1^2 + 6.04/D2^2)).
 const double D2_SYMBOL = 1088.0 / 180.0;
 const double RK3_REAL_LIMIT = 2.51;
-
 }  // namespace
-
-struct fg2_sim {
-  int n1 = 0, n2 = 0, storage = ST_F32;
-  Layout L{};
-  void *u[2] = {nullptr, nullptr};
-  void *v = nullptr;
-  int cur = 0;  // u[cur] holds the state
-  // substage descriptors: [0] u[0] -> u[1], [1] u[1] -> u[0], [2] the mirror API's kick
-  GridDesc *desc = nullptr;   // device
-  GridDesc desc_host[3];
-  bool desc_valid = false;
-  int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  Status *status = nullptr;       // device
-  Status *status_host = nullptr;  // pinned mirror
-  double *sums_partial = nullptr, *sums_out = nullptr;
-  double para[NPARA];  // runtime keys by slot, then the scheme's derived constants
-  double l1 = 1.0, l2 = 1.0, c = 0.5;  // src/global.cpp:28
-  int p1 = 1, p2 = 1;                  // src/global.cpp:29
-  double delta1 = 0, delta2 = 0;
-  bool configured = false;
-  bool ghosts_valid = false;
-  bool smax_valid = false;
-  int dt_mode = FG2_DT_REFERENCE;
-  Rng forcing{0x5eed5eedull};
-  bool fixed_phases = false;
-  float r1 = 0.f, r2 = 0.f;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step graph per ping-pong parity
-  double graph_dt[2] = {0, 0}, graph_tend[2] = {0, 0};
-  char para_msg[256];
-};
-
-namespace {
 
 size_t array_elems(const fg2_sim *s) { return (size_t)s->L.elems(); }
 
@@ -164,7 +119,6 @@ int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridD
   return FG2_OK;
 }
 
-bool supported_storage(int st) { return st == ST_F32 || st == ST_F64; }
 
 int ensure_config(fg2_sim *s)
 {
@@ -265,13 +219,17 @@ int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
 void drop_graph(fg2_sim *s)
 {
   s->desc_valid = false;
+  ++s->version;
   for (int b = 0; b < 2; ++b) {
     if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);
     s->graph[b] = nullptr;
   }
 }
 
-}  // namespace
+}  // namespace rt
+}  // namespace fg2
+
+using namespace fg2::rt;
 
 extern "C" {
 
@@ -302,17 +260,26 @@ int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, c
   return setup ? 1 : 0;
 }
 
-fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
+}  // extern "C"
+
+namespace fg2 {
+namespace rt {
+namespace {
+
+// A handle with the scheme's default parameters and its small device buffers (reduction
+// scratch, tile queue, descriptors); the caller sets or allocates the arrays.
+fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_arrays)
 {
   if (n1 < HALF || n2 < HALF) {
     fail(FG2_ERR_ARG, "grid %d x %d is smaller than the ghost width %d", n1, n2, HALF);
     return nullptr;
   }
-  if (!supported_storage(storage)) {
+  if (storage != ST_F32 && storage != ST_F64) {
     fail(FG2_ERR_UNSUPPORTED, "storage %d is not supported by the plain path", storage);
     return nullptr;
   }
   std::unique_ptr<fg2_sim> s(new fg2_sim);
+  s->own_arrays = own_arrays;
   s->n1 = n1;
   s->n2 = n2;
   s->storage = storage;
@@ -321,7 +288,7 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   for (int q = 0; q < scheme::NSLOT; ++q) s->para[scheme::PARA_KEYS[q].slot] = round_para(s.get(), scheme::PARA_KEYS[q].def);
   scheme::derive(s->para);
   if (stream) {
-    s->stream = (cudaStream_t)stream;
+    s->stream = stream;
   } else {
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
       fail(FG2_ERR_ALLOC, "stream creation failed");
@@ -329,32 +296,63 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
     }
     s->own_stream = true;
   }
-  const size_t bytes = array_elems(s.get()) * elem_size(storage);
-  auto cleanup = [&](const char *what) {
-    fail(FG2_ERR_ALLOC, "%s", what);
+  if (cudaMalloc(&s->sums_partial, sizeof(double) * 4 * sums_blocks(s->L)) != cudaSuccess ||
+      cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess || cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&s->desc, 3 * sizeof(GridDesc)) != cudaSuccess ||
+      cudaMemsetAsync(s->queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess) {
+    fail(FG2_ERR_ALLOC, "device allocation of the handle's buffers failed");
     fg2_sim_destroy(s.release());
     return nullptr;
-  };
+  }
+  return s.release();
+}
+
+}  // namespace
+
+fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, Status *status,
+                       Status *status_host)
+{
+  fg2_sim *s = new_handle(n1, n2, storage, stream, false);
+  if (!s) return nullptr;
+  s->u[0] = u0;
+  s->u[1] = u1;
+  s->v = v;
+  s->status = status;
+  s->status_host = status_host;
+  return s;
+}
+
+}  // namespace rt
+}  // namespace fg2
+
+extern "C" {
+
+fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
+{
+  std::unique_ptr<fg2_sim, void (*)(fg2_sim *)> s(new_handle(n1, n2, storage, (cudaStream_t)stream, true),
+                                                  fg2_sim_destroy);
+  if (!s) return nullptr;
+  const size_t bytes = array_elems(s.get()) * elem_size(storage);
   if (cudaMalloc(&s->u[0], bytes) != cudaSuccess || cudaMalloc(&s->u[1], bytes) != cudaSuccess ||
-      cudaMalloc(&s->v, bytes) != cudaSuccess)
-    return cleanup("device allocation of the state failed");
+      cudaMalloc(&s->v, bytes) != cudaSuccess) {
+    fail(FG2_ERR_ALLOC, "device allocation of the state failed");
+    return nullptr;
+  }
   if (cudaMalloc(&s->status, sizeof(Status)) != cudaSuccess ||
-      cudaMallocHost(&s->status_host, sizeof(Status)) != cudaSuccess)
-    return cleanup("status allocation failed");
-  if (cudaMalloc(&s->sums_partial, sizeof(double) * 4 * sums_blocks(s->L)) != cudaSuccess ||
-      cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess)
-    return cleanup("reduction scratch allocation failed");
-  if (cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess) return cleanup("queue allocation failed");
-  if (cudaMalloc(&s->desc, 3 * sizeof(GridDesc)) != cudaSuccess) return cleanup("descriptor allocation failed");
+      cudaMallocHost(&s->status_host, sizeof(Status)) != cudaSuccess) {
+    fail(FG2_ERR_ALLOC, "status allocation failed");
+    return nullptr;
+  }
   // every array starts at -max like the reference (src/setup.cpp:80-83)
   const double lowest = storage == ST_F64 ? -std::numeric_limits<double>::max() : -std::numeric_limits<float>::max();
   if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->u[1], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->v, array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       cudaMemsetAsync(s->status, 0, sizeof(Status), s->stream) != cudaSuccess ||
-      cudaMemsetAsync(s->queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess ||
-      cudaStreamSynchronize(s->stream) != cudaSuccess)
-    return cleanup("initial fill failed");
+      cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    fail(FG2_ERR_ALLOC, "initial fill failed");
+    return nullptr;
+  }
   return s.release();
 }
 
@@ -363,11 +361,13 @@ void fg2_sim_destroy(fg2_sim *s)
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graph(s);
-  cudaFree(s->u[0]);
-  cudaFree(s->u[1]);
-  cudaFree(s->v);
-  cudaFree(s->status);
-  cudaFreeHost(s->status_host);
+  if (s->own_arrays) {
+    cudaFree(s->u[0]);
+    cudaFree(s->u[1]);
+    cudaFree(s->v);
+    cudaFree(s->status);
+    cudaFreeHost(s->status_host);
+  }
   cudaFree(s->sums_partial);
   cudaFree(s->sums_out);
   cudaFree(s->queue);

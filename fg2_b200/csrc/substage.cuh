@@ -3,9 +3,10 @@
 //
 // Work decomposition.  A launch advances a list of grids (one simulation, or a batch of
 // independent simulations of any sizes).  A tile is a strip of SW = 128 interior columns by
-// TH = 35 rows of one grid; the launch's tiles are numbered grid by grid, strip fastest, and a
-// persistent grid of CTAs drains them from a queue (an atomic counter that the last CTA to
-// finish resets, so a launch needs no host-side reset and replays from a CUDA graph).  A CTA
+// 7 nb rows of one grid (nb blocks of 7 output rows, a launch parameter, 5 by default); the
+// launch's tiles are numbered grid by grid, strip fastest, and a persistent grid of CTAs
+// drains them from a queue (an atomic counter that the last CTA to finish resets, so a launch
+// needs no host-side reset and replays from a CUDA graph).  A CTA
 // has 4 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in
 // device memory: its TMA tensor maps, output pointers, layout, boundaries, time step and
 // status block.
@@ -43,9 +44,6 @@
 
 namespace sub {
 
-#ifndef FG2_NB
-#define FG2_NB 5
-#endif
 #ifndef FG2_NSLOT
 #define FG2_NSLOT 2
 #endif
@@ -53,8 +51,7 @@ namespace sub {
 constexpr int SW = 128;            // interior columns per tile (strip width)
 constexpr int BW = SW + 2 * GL;    // TMA box width of u (halo 4 + 4; the stencil uses 3)
 constexpr int CH = 7;              // rows per chunk = register window period
-constexpr int NB = FG2_NB;         // output blocks per tile
-constexpr int TH = NB * CH;        // output rows per tile
+constexpr int NB_DEFAULT = TILE_BLOCKS_DEFAULT;  // output blocks per tile unless a launch sets nb
 constexpr int NCW = 4;             // warps per CTA
 constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
 constexpr int NP = (NV + 1) / 2;   // field pairs
@@ -121,11 +118,12 @@ struct TileGrid {
   int strips, rows, ntiles;
 };
 
-__host__ __device__ inline TileGrid tile_grid(const Layout &L)
+__host__ __device__ inline TileGrid tile_grid(const Layout &L, int nb)
 {
   TileGrid g;
+  const int th = nb * CH;
   g.strips = (L.n2 + SW - 1) / SW;
-  g.rows = (L.n1 + TH - 1) / TH;
+  g.rows = (L.n1 + th - 1) / th;
   g.ntiles = g.strips * g.rows;
   return g;
 }
@@ -332,7 +330,8 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 // Issues the next chunk of the CTA's sequence into its slot (free by the caller's check).
 template <class T, bool READ_V>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
-                                            int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int *queue)
+                                            int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
+                                            int *queue)
 {
   using G = Geo<T, READ_V>;
   if (ps->done) return;
@@ -346,7 +345,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
       const int g = grid_of_tile(grids, ngrids, t);
       const int local = t - grids[g].tile0, strips = grids[g].strips;
       ps->g = g;
-      ps->i0 = (local / strips) * TH;
+      ps->i0 = (local / strips) * (nb * CH);
       ps->j0 = (local % strips) * SW;
       grid_of[s] = g;
     }
@@ -366,7 +365,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     if (with_v)
       tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL) / G::G,
                   i0 + CH * (c - 1) + GT);
-    ps->c = c == NB ? 0 : c + 1;
+    ps->c = c == nb ? 0 : c + 1;
   }
   ps->next_n = n + 1;
 }
@@ -438,7 +437,7 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, queue);
+    for (int s = 0; s < NS; ++s) issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
   }
   __syncthreads();
 
@@ -470,7 +469,7 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
         cur_g = g;
       }
       const int local = tile - grids[g].tile0, strips = grids[g].strips;
-      i0 = (local / strips) * TH;
+      i0 = (local / strips) * (a.nb * CH);
       j0 = (local % strips) * SW;
 #pragma unroll
       for (int g2 = 0; g2 < 2; ++g2)
@@ -499,9 +498,9 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, queue);  // refill slot s
+      issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
     ++n;
-    b = b == NB - 1 ? -1 : b + 1;
+    b = b == a.nb - 1 ? -1 : b + 1;
   }
 
   if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);

@@ -136,6 +136,40 @@ void *fg2_sim_stream(fg2_sim *s);
 int fg2_sim_dump(fg2_sim *s, const char *path, double time);
 int fg2_sim_load(fg2_sim *s, const char *path, double *time);
 
+/* ---- batches of independent simulations --------------------------------------------------
+ * No single counterpart in the reference, which advances one grid per process
+ * (src/main.cpp:81-116).  A batch owns count members of any sizes (n1[k] x n2[k]) in one
+ * device arena and advances them together: one persistent substage launch per RK3 stage over
+ * the tiles of every member.  Members are ordinary handles (fg2_batch_member) for init,
+ * upload/download, sums, time, dump/load and per-member status; they belong to the batch
+ * (never fg2_sim_destroy them) and share its stream.  All members must hold the same scheme
+ * parameters (fg2_batch_para sets them on every member); box, boundaries and Courant number
+ * may differ per member. */
+typedef struct fg2_batch fg2_batch;
+fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage, void *stream);
+void fg2_batch_destroy(fg2_batch *b);
+int fg2_batch_count(const fg2_batch *b);
+long long fg2_batch_cells(const fg2_batch *b);     /* sum of n1[k] n2[k] */
+size_t fg2_batch_device_bytes(const fg2_batch *b); /* the arena of u, u', v */
+void *fg2_batch_stream(fg2_batch *b);
+fg2_sim *fg2_batch_member(fg2_batch *b, int k);
+int fg2_batch_set_box(fg2_batch *b, double l1, double l2);  /* every member */
+int fg2_batch_set_courant(fg2_batch *b, double c);
+int fg2_batch_set_bcond(fg2_batch *b, int p1, int p2);
+const char *fg2_batch_para(fg2_batch *b, const char *kv);
+int fg2_batch_config(fg2_batch *b);
+int fg2_batch_set_time(fg2_batch *b, double t);
+/* nsteps RK3 steps of every member.  dt > 0: that step for all; dt <= 0: each member's own
+ * CFL step, device-resident, capped at t_end.  use_graph: replay two captured steps. */
+int fg2_batch_advance(fg2_batch *b, int nsteps, double dt, double t_end, int use_graph);
+int fg2_batch_sync(fg2_batch *b); /* wait; worst status over the members */
+/* Tiling of the batch launches: tile height in blocks of 7 rows (nb) and CTAs per SM
+ * (0: as many as fit).  fg2_batch_autotune times steps of each candidate on the batch's own
+ * members (with dt = 0, which leaves every state unchanged) and keeps the fastest. */
+int fg2_batch_set_tiling(fg2_batch *b, int nb, int ctas_per_sm);
+int fg2_batch_get_tiling(const fg2_batch *b, int *nb, int *ctas_per_sm);
+int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms);
+
 /* ---- allocation-free sums ---------------------------------------------------------------
  * No counterpart in the reference.  The FP64 sums of fg2_sim_sums for callers that cannot
  * call cudaMalloc (their allocator already holds the GPU's memory, or the call sits in a
