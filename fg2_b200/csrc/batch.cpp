@@ -455,59 +455,57 @@ int fg2_batch_sync(fg2_batch *b)
 }
 
 // Times steps of every candidate tiling with dt = 0 (u' = u + 0 v leaves every member's state
-// unchanged; v is dead between steps) and keeps the fastest.
+// unchanged; v is dead between steps) and keeps the fastest: every candidate once, then the
+// three best again, each candidate scored by its faster measurement.
 int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
 {
   if (!b || reps < 1) return fail(FG2_ERR_ARG, "bad arguments");
   int rc = check_members(b);
   if (rc) return rc;
-  static const int NBS[] = {2, 3, 4, 5, 6, 8};
-  const int ctas_max = 3;
+  struct Cand {
+    int nb, ctas;
+    double ms;
+  };
+  std::vector<Cand> cands;
+  for (int nb : {2, 3, 4, 5, 6, 8})
+    for (int ctas = 1; ctas <= 3; ++ctas) cands.push_back({nb, ctas, std::numeric_limits<double>::infinity()});
   const int keep_nb = b->nb, keep_ctas = b->max_ctas;
-  double best = std::numeric_limits<double>::infinity();
-  int best_nb = keep_nb, best_ctas = keep_ctas;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   rc = prepare_members(b, false);
-  for (int nb : NBS) {
-    for (int ctas = 1; ctas <= ctas_max && rc == 0; ++ctas) {
-      b->nb = nb;
-      b->max_ctas = ctas;
-      if ((rc = ensure_batch_descs(b, false)) != 0) break;
-      int set = 0;
-      // two untimed steps, then 2 reps timed (even counts leave the descriptor set at 0)
-      for (int r = 0; r < 2 && rc == 0; ++r) rc = enqueue_batch_step(b, 0.0, false, 0.0, set);
-      if (rc) break;
-      if (cudaEventRecord(e0, b->stream) != cudaSuccess) {
-        rc = fail(FG2_ERR_ARG, "event record failed");
-        break;
-      }
-      for (int r = 0; r < 2 * reps && rc == 0; ++r) rc = enqueue_batch_step(b, 0.0, false, 0.0, set);
-      if (rc) break;
-      float ms = 0.f;
-      if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        rc = fail(FG2_ERR_ARG, "autotune timing failed");
-        break;
-      }
-      const double per = ms / (2.0 * reps);
-      if (per < best) {
-        best = per;
-        best_nb = nb;
-        best_ctas = ctas;
-      }
-    }
-    if (rc) break;
+  auto measure = [&](Cand &c) -> int {
+    b->nb = c.nb;
+    b->max_ctas = c.ctas;
+    int r = ensure_batch_descs(b, false);
+    int set = 0;
+    // two untimed steps, then 2 reps timed (even counts leave the descriptor set at 0)
+    for (int q = 0; q < 2 && r == 0; ++q) r = enqueue_batch_step(b, 0.0, false, 0.0, set);
+    if (r) return r;
+    if (cudaEventRecord(e0, b->stream) != cudaSuccess) return fail(FG2_ERR_ARG, "event record failed");
+    for (int q = 0; q < 2 * reps && r == 0; ++q) r = enqueue_batch_step(b, 0.0, false, 0.0, set);
+    if (r) return r;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return fail(FG2_ERR_ARG, "autotune timing failed");
+    c.ms = std::min(c.ms, ms / (2.0 * reps));
+    return FG2_OK;
+  };
+  for (size_t i = 0; i < cands.size() && rc == 0; ++i) rc = measure(cands[i]);
+  if (rc == 0) {
+    std::sort(cands.begin(), cands.end(), [](const Cand &x, const Cand &y) { return x.ms < y.ms; });
+    for (size_t i = 0; i < 3 && i < cands.size() && rc == 0; ++i) rc = measure(cands[i]);
+    std::sort(cands.begin(), cands.end(), [](const Cand &x, const Cand &y) { return x.ms < y.ms; });
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->nb = rc ? keep_nb : best_nb;
-  b->max_ctas = rc ? keep_ctas : best_ctas;
+  b->nb = rc ? keep_nb : cands[0].nb;
+  b->max_ctas = rc ? keep_ctas : cands[0].ctas;
   drop_batch_graph(b);
   b->desc_valid = false;
   if (rc) return rc;
-  if (best_ms) *best_ms = best;
+  if (best_ms) *best_ms = cands[0].ms;
   return fg2_batch_sync(b);
 }
 
