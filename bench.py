@@ -318,6 +318,80 @@ def run_batch_leg(steps, warmup, device):
             "gpu_launches_per_step": 4}
 
 
+# ---- the 16-bit deviation-storage path (secondary results) ----------------------------------
+B_ALG_F16 = 10 * NVAR * 2  # 80 B per cell-step: hydro, 16-bit u and v
+
+
+def run_mixed_leg(state, steps, warmup, device, plain_value):
+    """The headline workload with the state stored as FP16 / BF16 deviations (per-field
+    background, per-64x64-tile scales), FP32 stencil, residual-carrying update."""
+    import torch
+    import fg2_b200
+    out = {}
+    peak, _ = peaks()
+    for storage in ("f16", "bf16"):
+        sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=storage)
+        sim.config()
+        sim.upload(state)
+        sim.set_dt_mode("cfl")
+        stream = torch.cuda.ExternalStream(sim.stream, device=device)
+        sim.set_time(0.0)
+        sim.advance(max(warmup, 3), 0.0, graph=True)
+        if sim.sync() != 0:
+            raise RuntimeError(f"{storage} warm-up produced a bad status")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.advance(steps, 0.0, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        status = sim.sync()
+        sim.close()
+        value = N1 * N2 * steps / (ms / 1e3) / 1e9
+        out[storage] = {"value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps, "status": status,
+                        "speedup_vs_plain_f32": value / plain_value,
+                        "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_F16, "achieved": value * B_ALG_F16,
+                                     "peak": peak, "unit": "GB/s", "frac": value * B_ALG_F16 / peak}}
+    return out
+
+
+def run_precision_leg(n, steps, device):
+    """Kelvin-Helmholtz at n x n, the same fixed step sequence in FP64, FP32 and the 16-bit
+    deviation storages; per-field L2 (RMS) and Linf errors against the FP64 run, and the
+    relative L2 error of the density rho = exp(lnd)."""
+    import fg2_b200
+    state = fg2_b200.setup_evaluate(SETUP, n, n, SCHEME, seed=SEED)[0]
+    with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f64") as s:
+        s.config()
+        s.upload(state)
+        s.set_dt_mode("cfl")
+        dt = 0.9 * s.getdt()
+        s.advance(steps, dt)
+        ref = s.download()
+    state32 = state.astype(np.float32)
+    del state
+    rho_ref = np.exp(ref[..., 0])
+    rho_norm = np.sqrt((rho_ref ** 2).sum())
+    result = {"grid": [n, n], "steps": steps, "dt": dt, "fields": ["lnd", "u1", "u2", "lne"]}
+    for storage in ("f32", "f16", "bf16"):
+        with fg2_b200.Sim(n, n, scheme=SCHEME, storage=storage) as s:
+            s.config()
+            s.upload(state32)
+            s.advance(steps, dt)
+            status = s.sync()
+            out = s.download()
+        err = out.astype(np.float64) - ref
+        rms = np.sqrt((err.reshape(-1, NVAR) ** 2).mean(0))
+        linf = np.abs(err.reshape(-1, NVAR)).max(0)
+        rho_l2 = float(np.sqrt(((np.exp(out[..., 0].astype(np.float64)) - rho_ref) ** 2).sum()) / rho_norm)
+        result[storage] = {"status": status, "l2_rms": rms.tolist(), "linf": linf.tolist(), "rho_rel_l2": rho_l2}
+        del out, err
+    for storage in ("f16", "bf16"):
+        result[storage]["rho_rel_l2_vs_f32"] = result[storage]["rho_rel_l2"] / max(result["f32"]["rho_rel_l2"], 1e-300)
+    return result
+
+
 def run_fused(args):
     import torch
     import fg2_b200
@@ -384,6 +458,11 @@ def run_fused(args):
     if rank == 0 and world == 1 and not args.no_batch:
         batch = run_batch_leg(200, args.warmup, device)
 
+    mixed, precision = None, None
+    if rank == 0 and world == 1 and not args.no_mixed:
+        mixed = run_mixed_leg(state, args.steps, args.warmup, device, value / world)
+        precision = run_precision_leg(8192, 500, device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
@@ -410,6 +489,8 @@ def run_fused(args):
             "cpu_baseline": cpu,
             "e2e": e2e, "e2e_status": e2e_status,
             "batch": batch,
+            "mixed": mixed,
+            "precision": precision,
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }
@@ -428,6 +509,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch (secondary) leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the 16-bit storage and precision legs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -98,7 +98,7 @@ int ensure_batch_descs(fg2_batch *b, bool device_dt)
     for (int set = 0; set < 2; ++set) {
       const int in = set == 0 ? m->cur : 1 - m->cur;
       if (make_grid_desc(&b->desc_host[(size_t)set * b->count + r], m->u[in], m->u[1 - in], m->v, m->L, m->storage,
-                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0) != CUDA_SUCCESS)
+                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0, dev_code(m)) != CUDA_SUCCESS)
         return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed for batch member %d", k);
     }
     tile0 += substage_tiles(m->L, b->nb);
@@ -136,6 +136,7 @@ int enqueue_batch_step(fg2_batch *b, double dt, bool device_dt, double t_end, in
     a.status = b->status;
     a.nb = b->nb;
     a.max_ctas = b->max_ctas;
+    a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
     CK(launch_substage(b->storage, kind, device_dt && k == 2, true, b->desc + (size_t)set * b->count, b->count,
                        b->ntiles, a, b->queue, b->stream));
@@ -165,7 +166,8 @@ int prepare_members(fg2_batch *b, bool device_dt)
     }
     if (device_dt && !m->smax_valid) {
       CK(cudaMemsetAsync(&m->status->smax, 0, sizeof(unsigned long long), b->stream));
-      CK(launch_signal_max(m->storage, m->u[m->cur], m->L, m->para, m->delta1, m->delta2, m->status, b->stream));
+      CK(launch_signal_max(m->storage, m->u[m->cur], m->L, m->para, m->delta1, m->delta2, m->status, b->stream,
+                           dev_code(m)));
       m->smax_valid = true;
     }
   }
@@ -213,8 +215,8 @@ fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage
     fail(FG2_ERR_ARG, "a batch needs at least one member");
     return nullptr;
   }
-  if (storage != ST_F32 && storage != ST_F64) {
-    fail(FG2_ERR_UNSUPPORTED, "storage %d is not supported by the batch path", storage);
+  if (storage != ST_F32 && storage != ST_F64 && storage != ST_F16 && storage != ST_BF16) {
+    fail(FG2_ERR_UNSUPPORTED, "unknown storage %d", storage);
     return nullptr;
   }
   for (int k = 0; k < count; ++k)

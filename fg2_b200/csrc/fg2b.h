@@ -111,6 +111,19 @@ struct Status {
 };
 enum ErrorBits : unsigned { ERR_TMA_TIMEOUT = 1u, ERR_QUEUE_TIMEOUT = 2u };
 
+// Deviation storage (FP16 / BF16 state arrays).  A stored 16-bit number h of field f stands
+// for bg[f] + s h, with s the scale of field f on the SCALE_TILE x SCALE_TILE tile of the
+// interior cell that holds the value (a ghost cell uses the tile of the interior cell it
+// images).  Fields whose sign flips at a reflecting wall have bg = 0, so a ghost image is the
+// negated 16-bit number.  v (the RK3 register) is stored as plain 16-bit numbers.
+constexpr int SCALE_TILE = 64;
+struct DevCode {
+  float bg[4];           // per-field background (field mean at upload)
+  const float4 *scale;   // per tile, row-major over (n1 / 64, n2 / 64) tiles: s of each field
+  const float4 *inv;     // per tile: 1 / s
+  int tiles2;            // tiles along axis 2
+};
+
 // ---- arithmetic on a scalar or on a pair of cells ------------------------------------------
 // The fused kernel evaluates two cells per thread; for FP32 the pair is a float2 and every
 // operation is one packed sm_100 instruction (add/mul/fma .f32x2), for FP64 a double2

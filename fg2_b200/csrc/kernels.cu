@@ -14,6 +14,8 @@
 // u is ping-ponged between two arrays so no stage overwrites a halo another tile reads.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -47,6 +49,34 @@ struct PairOf<double> {
   static __host__ __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
 };
 
+// Storage types of the state arrays: the compute type C and, for 16-bit deviation storage
+// (DEV), conversions of single values and of packed pairs.
+template <class S>
+struct Store {
+  using C = S;
+  static constexpr bool DEV = false;
+};
+template <>
+struct Store<__half> {
+  using C = float;
+  using S2 = __half2;
+  static constexpr bool DEV = true;
+  static __device__ __forceinline__ float to(__half h) { return __half2float(h); }
+  static __device__ __forceinline__ __half from(float x) { return __float2half_rn(x); }
+  static __device__ __forceinline__ float2 to2(__half2 h) { return __half22float2(h); }
+  static __device__ __forceinline__ __half2 from2(float2 x) { return __float22half2_rn(x); }
+};
+template <>
+struct Store<__nv_bfloat16> {
+  using C = float;
+  using S2 = __nv_bfloat162;
+  static constexpr bool DEV = true;
+  static __device__ __forceinline__ float to(__nv_bfloat16 h) { return __bfloat162float(h); }
+  static __device__ __forceinline__ __nv_bfloat16 from(float x) { return __float2bfloat16_rn(x); }
+  static __device__ __forceinline__ float2 to2(__nv_bfloat162 h) { return __bfloat1622float2(h); }
+  static __device__ __forceinline__ __nv_bfloat162 from2(float2 x) { return __float22bfloat162_rn(x); }
+};
+
 // Parameters of one substage launch, rounded to the storage precision T: the stencil
 // weights both as scalars and broadcast to both lanes of a pair (so packed instructions read
 // them straight from the constant bank), the scheme's parameters as scalars.
@@ -61,6 +91,7 @@ struct KParams {
   const double *dt_dev;  // device time step for grids without their own, or null: dt
   Status *status;        // launch errors
   int nb;                // output blocks of 7 rows per tile
+  double comp_bg;        // beta * gamma of the next stage (16-bit residual carry), or 0
 };
 
 template <class T>
@@ -115,6 +146,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.dt_dev = a.dt_dev;
   kp.status = a.status;
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
+  kp.comp_bg = a.comp_bg;
   return kp;
 }
 
@@ -209,7 +241,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
 // Cells per 16-byte group: TMA boxes are built from whole groups, so the innermost box
 // dimension (one group of interleaved cells, NV x 16 bytes) is a 16-byte multiple for any
 // NVAR and the innermost coordinate is always 0.
-int group_cells(int storage) { return storage == ST_F64 ? 2 : storage == ST_F32 ? 4 : 8; }
+int elem_bytes(int storage) { return storage == ST_F64 ? 8 : storage == ST_F32 ? 4 : 2; }
+int group_cells(int storage) { return sub::group_of(elem_bytes(storage)); }
 
 // Map over the padded array as (group element, cell group, padded row): box_cells x box_rows
 // boxes land in shared memory as [row][cell][field]; the map covers ext_cells cells (whole
@@ -219,7 +252,7 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
 {
   PFN_cuTensorMapEncodeTiled_v12000 encode = encoder();
   if (!encode) return CUDA_ERROR_NOT_FOUND;
-  const size_t elem = storage == ST_F64 ? 8 : (storage == ST_F32 ? 4 : 2);
+  const size_t elem = elem_bytes(storage);
   const int G = group_cells(storage);
   const CUtensorMapDataType dt = storage == ST_F64   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                  : storage == ST_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
@@ -235,11 +268,14 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
 }  // namespace
 
 CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
-                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0)
+                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0,
+                        const DevCode *dev)
 {
   CUresult r = encode_map(&d->tm_u, u_in, L, storage, sub::BW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
-  r = encode_map(&d->tm_v, v, L, storage, sub::SW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+  // the v box starts GL % G cells left of the strip when a cell group is wider than GL
+  const int G = group_cells(storage), vbw = (sub::SW + GL % G + G - 1) / G * G;
+  r = encode_map(&d->tm_v, v, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
   d->u_out = u_out;
   d->v = v;
@@ -256,17 +292,19 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   d->inv22 = 1.0 / (delta2 * delta2);
   d->inv12 = 1.0 / (delta1 * delta2);
   d->delta1 = delta1;
+  if (dev) d->dev = *dev;
+  else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0};
   return CUDA_SUCCESS;
 }
 
 int substage_tiles(const Layout &L, int nb) { return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT).ntiles; }
 
-template <class T, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
-static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<T> &kp, int max_ctas,
-                                int *queue, cudaStream_t s)
+template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
+static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
+                                int max_ctas, int *queue, cudaStream_t s)
 {
-  using G = sub::Geo<T, RV>;
-  auto kern = sub::substage_kernel<T, M2, RV, WV, WU, CF, SC>;
+  using G = sub::Geo<S, RV>;
+  auto kern = sub::substage_kernel<S, M2, RV, WV, WU, CF, SC>;
   static int ctas_per_sm = 0, sms = 0;
   if (!ctas_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
@@ -285,17 +323,17 @@ static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, c
   return cudaGetLastError();
 }
 
-template <class T, unsigned M2, bool SC>
-static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int nt, const KParams<T> &kp, int mc,
-                              int *queue, cudaStream_t s)
+template <class S, unsigned M2, bool SC>
+static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int nt,
+                              const KParams<typename Store<S>::C> &kp, int mc, int *queue, cudaStream_t s)
 {
   switch (kind) {
-    case STAGE_FIRST: return run_substage<T, M2, false, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
-    case STAGE_MID: return run_substage<T, M2, true, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
+    case STAGE_FIRST: return run_substage<S, M2, false, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
+    case STAGE_MID: return run_substage<S, M2, true, true, true, false, SC>(g, ng, nt, kp, mc, queue, s);
     case STAGE_LAST:
-      return cfl ? run_substage<T, M2, true, false, true, true, SC>(g, ng, nt, kp, mc, queue, s)
-                 : run_substage<T, M2, true, false, true, false, SC>(g, ng, nt, kp, mc, queue, s);
-    case STAGE_KICK: return run_substage<T, M2, true, true, false, false, SC>(g, ng, nt, kp, mc, queue, s);
+      return cfl ? run_substage<S, M2, true, false, true, true, SC>(g, ng, nt, kp, mc, queue, s)
+                 : run_substage<S, M2, true, false, true, false, SC>(g, ng, nt, kp, mc, queue, s);
+    case STAGE_KICK: return run_substage<S, M2, true, true, false, false, SC>(g, ng, nt, kp, mc, queue, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -303,27 +341,37 @@ static cudaError_t substage_m(int kind, bool cfl, const GridDesc *g, int ng, int
 // The kernels are compiled for two sets of second-derivative fields: the scheme's default
 // parameters' set, and all fields (correct for any parameters: an unused D11/D22 meets a
 // zero coefficient).  FP64, the reference-precision path, always uses all fields.
-template <class T, bool SC>
+template <class S, bool SC>
 static cudaError_t substage_t(int kind, bool cfl, const GridDesc *g, int ng, int nt, const StageArgs &a, int *queue,
                               cudaStream_t s)
 {
+  using T = typename Store<S>::C;
   const KParams<T> kp = make_params<T>(a, SC);
   const unsigned need = scheme::d2_fields(a.para);
   if constexpr (sizeof(T) == 4) {
-    if ((need & ~scheme::D2_DEFAULT) == 0) return substage_m<T, scheme::D2_DEFAULT, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
+    if ((need & ~scheme::D2_DEFAULT) == 0)
+      return substage_m<S, scheme::D2_DEFAULT, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
   }
-  return substage_m<T, scheme::D2_ALL, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
+  return substage_m<S, scheme::D2_ALL, SC>(kind, cfl, g, ng, nt, kp, a.max_ctas, queue, s);
+}
+
+template <class S>
+static cudaError_t substage_s(int kind, bool cfl, bool scaled, const GridDesc *grids, int ngrids, int ntiles,
+                              const StageArgs &a, int *queue, cudaStream_t s)
+{
+  return scaled ? substage_t<S, true>(kind, cfl, grids, ngrids, ntiles, a, queue, s)
+                : substage_t<S, false>(kind, cfl, grids, ngrids, ntiles, a, queue, s);
 }
 
 cudaError_t launch_substage(int storage, int kind, bool cfl, bool scaled, const GridDesc *grids, int ngrids,
                             int ntiles, const StageArgs &a, int *queue, cudaStream_t s)
 {
-  if (storage == ST_F32)
-    return scaled ? substage_t<float, true>(kind, cfl, grids, ngrids, ntiles, a, queue, s)
-                  : substage_t<float, false>(kind, cfl, grids, ngrids, ntiles, a, queue, s);
-  if (storage == ST_F64)
-    return scaled ? substage_t<double, true>(kind, cfl, grids, ngrids, ntiles, a, queue, s)
-                  : substage_t<double, false>(kind, cfl, grids, ngrids, ntiles, a, queue, s);
+  switch (storage) {
+    case ST_F32: return substage_s<float>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+    case ST_F64: return substage_s<double>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+    case ST_F16: return substage_s<__half>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+    case ST_BF16: return substage_s<__nv_bfloat16>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+  }
   return cudaErrorInvalidValue;
 }
 
@@ -403,10 +451,23 @@ __global__ void fill_kernel(T *p, size_t n, T x)
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) p[k] = x;
 }
 
+// Value of field f at interior cell (i, j), decoded for 16-bit deviation storage.
+template <class S>
+__device__ __forceinline__ double value_at(const S *u, const Layout &L, const DevCode &dc, int f, int i, int j)
+{
+  if constexpr (!Store<S>::DEV) {
+    return (double)u[L.at(f, i, j)];
+  } else {
+    const float4 sc = __ldg(dc.scale + (i / SCALE_TILE) * dc.tiles2 + j / SCALE_TILE);
+    const float sf = f == 0 ? sc.x : f == 1 ? sc.y : f == 2 ? sc.z : sc.w;
+    return (double)fmaf(sf, Store<S>::to(u[L.at(f, i, j)]), dc.bg[f]);
+  }
+}
+
 // getdt's reduction in FP64: max over cells of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
 template <class T>
 __global__ void signal_max_kernel(const T *u, const Layout L, const Para<double> p, double inv1, double inv2,
-                                  Status *st)
+                                  Status *st, const DevCode dc)
 {
   const long long n = (long long)L.n1 * L.n2;
   double m = 0.0;
@@ -414,7 +475,7 @@ __global__ void signal_max_kernel(const T *u, const Layout L, const Para<double>
     const int i = (int)(k / L.n2), j = (int)(k % L.n2);
     double q[NV];
 #pragma unroll
-    for (int f = 0; f < NV; ++f) q[f] = (double)u[L.at(f, i, j)];
+    for (int f = 0; f < NV; ++f) q[f] = value_at<T>(u, L, dc, f, i, j);
     const double cs = scheme::sound_speed<double>(q, p);
     m = fmax(m, (fabs(q[scheme::U1]) + cs) * inv1 + (fabs(q[scheme::U2]) + cs) * inv2);
   }
@@ -430,7 +491,7 @@ constexpr int SUM_THREADS = 256;
 int sums_blocks(const Layout &L) { return L.n1 < 1024 ? L.n1 : 1024; }
 
 template <class T>
-__global__ void sums_kernel(const T *u, const Layout L, double *partials)
+__global__ void sums_kernel(const T *u, const Layout L, double *partials, const DevCode dc)
 {
   __shared__ double red[4][SUM_THREADS];
   double acc[4] = {0, 0, 0, 0};
@@ -438,7 +499,7 @@ __global__ void sums_kernel(const T *u, const Layout L, double *partials)
     for (int j = threadIdx.x; j < L.n2; j += blockDim.x) {
       double q[NV], c[4];
 #pragma unroll
-      for (int f = 0; f < NV; ++f) q[f] = (double)u[L.at(f, i, j)];
+      for (int f = 0; f < NV; ++f) q[f] = value_at<T>(u, L, dc, f, i, j);
       scheme::conserved(q, c);
 #pragma unroll
       for (int k = 0; k < 4; ++k) acc[k] += c[k];
@@ -488,6 +549,39 @@ __global__ void dt_update_kernel(Status *st, double courant, double dt_diff, dou
   st->steps += 1ull;
 }
 
+// Deviation storage: FP32 cells (n1 x n2 x NV, no ghosts) -> 16-bit numbers, the
+// substage kernel's encoding (h = (x - bg) / s of the cell's tile, rounded once).
+template <class S>
+__global__ void encode_kernel(S *u, const float *src, const Layout L, const DevCode dc, bool with_code)
+{
+  const long long n = (long long)L.n1 * L.n2 * NV;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(k % NV);
+    const long long cell = k / NV;
+    const int i = (int)(cell / L.n2), j = (int)(cell % L.n2);
+    if (!with_code) {
+      u[L.at(f, i, j)] = Store<S>::from(src[k]);
+      continue;
+    }
+    const float4 iv = __ldg(dc.inv + (i / SCALE_TILE) * dc.tiles2 + j / SCALE_TILE);
+    const float inv = f == 0 ? iv.x : f == 1 ? iv.y : f == 2 ? iv.z : iv.w;
+    u[L.at(f, i, j)] = Store<S>::from((src[k] - dc.bg[f]) * inv);
+  }
+}
+
+// 16-bit numbers -> FP32 cells; with_code false: plain conversion (v).
+template <class S>
+__global__ void decode_kernel(float *dst, const S *u, const Layout L, const DevCode dc, bool with_code)
+{
+  const long long n = (long long)L.n1 * L.n2 * NV;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(k % NV);
+    const long long cell = k / NV;
+    const int i = (int)(cell / L.n2), j = (int)(cell % L.n2);
+    dst[k] = with_code ? (float)value_at<S>(u, L, dc, f, i, j) : Store<S>::to(u[L.at(f, i, j)]);
+  }
+}
+
 // Device-resident time steps of a batch: member k takes min(courant_k / smax_k, dt_diff_k),
 // capped at t_end, exactly as dt_update_kernel does for one simulation.
 __global__ void dt_update_batch_kernel(Status *st, const double2 *limits, int count, double t_end)
@@ -523,6 +617,8 @@ cudaError_t launch_bcond(int storage, void *u, const Layout &L, int p1, int p2, 
   const int g = (int)((n + 255) / 256);
   if (storage == ST_F32) bcond_kernel<float><<<g, 256, 0, s>>>((float *)u, L, p1, p2);
   else if (storage == ST_F64) bcond_kernel<double><<<g, 256, 0, s>>>((double *)u, L, p1, p2);
+  else if (storage == ST_F16) bcond_kernel<__half><<<g, 256, 0, s>>>((__half *)u, L, p1, p2);
+  else if (storage == ST_BF16) bcond_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((__nv_bfloat16 *)u, L, p1, p2);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -560,32 +656,68 @@ cudaError_t launch_fill(int storage, void *p, size_t count, double value, cudaSt
   const int g = grid_for((long long)count, 256);
   if (storage == ST_F32) fill_kernel<float><<<g, 256, 0, s>>>((float *)p, count, (float)value);
   else if (storage == ST_F64) fill_kernel<double><<<g, 256, 0, s>>>((double *)p, count, value);
+  else if (storage == ST_F16 || storage == ST_BF16) return cudaMemsetAsync(p, 0, count * 2, s);  // 16-bit: h = 0
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const double *para, double delta1,
-                              double delta2, Status *st, cudaStream_t s)
+                              double delta2, Status *st, cudaStream_t s, const DevCode *dev)
 {
   const int g = grid_for((long long)L.n1 * L.n2, 256);
   Para<double> p;
   for (int q = 0; q < NPARA; ++q) p.v[q] = para[q];
-  if (storage == ST_F32)
-    signal_max_kernel<float><<<g, 256, 0, s>>>((const float *)u, L, p, 1.0 / delta1, 1.0 / delta2, st);
-  else if (storage == ST_F64)
-    signal_max_kernel<double><<<g, 256, 0, s>>>((const double *)u, L, p, 1.0 / delta1, 1.0 / delta2, st);
-  else
-    return cudaErrorInvalidValue;
+  const DevCode dc = dev ? *dev : DevCode{};
+  const double i1 = 1.0 / delta1, i2 = 1.0 / delta2;
+  switch (storage) {
+    case ST_F32: signal_max_kernel<float><<<g, 256, 0, s>>>((const float *)u, L, p, i1, i2, st, dc); break;
+    case ST_F64: signal_max_kernel<double><<<g, 256, 0, s>>>((const double *)u, L, p, i1, i2, st, dc); break;
+    case ST_F16: signal_max_kernel<__half><<<g, 256, 0, s>>>((const __half *)u, L, p, i1, i2, st, dc); break;
+    case ST_BF16:
+      signal_max_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16 *)u, L, p, i1, i2, st, dc);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *partials, double *out, cudaStream_t s)
+cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *partials, double *out, cudaStream_t s,
+                        const DevCode *dev)
 {
   const int nb = sums_blocks(L);
-  if (storage == ST_F32) sums_kernel<float><<<nb, SUM_THREADS, 0, s>>>((const float *)u, L, partials);
-  else if (storage == ST_F64) sums_kernel<double><<<nb, SUM_THREADS, 0, s>>>((const double *)u, L, partials);
-  else return cudaErrorInvalidValue;
+  const DevCode dc = dev ? *dev : DevCode{};
+  switch (storage) {
+    case ST_F32: sums_kernel<float><<<nb, SUM_THREADS, 0, s>>>((const float *)u, L, partials, dc); break;
+    case ST_F64: sums_kernel<double><<<nb, SUM_THREADS, 0, s>>>((const double *)u, L, partials, dc); break;
+    case ST_F16: sums_kernel<__half><<<nb, SUM_THREADS, 0, s>>>((const __half *)u, L, partials, dc); break;
+    case ST_BF16:
+      sums_kernel<__nv_bfloat16><<<nb, SUM_THREADS, 0, s>>>((const __nv_bfloat16 *)u, L, partials, dc);
+      break;
+    default: return cudaErrorInvalidValue;
+  }
   sums_final_kernel<<<1, SUM_THREADS, 0, s>>>(partials, nb, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_encode(int storage, void *u, const float *src, const Layout &L, const DevCode *dev, cudaStream_t s)
+{
+  const int g = grid_for((long long)L.n1 * L.n2 * NV, 256);
+  const DevCode dc = dev ? *dev : DevCode{};
+  if (storage == ST_F16) encode_kernel<__half><<<g, 256, 0, s>>>((__half *)u, src, L, dc, dev != nullptr);
+  else if (storage == ST_BF16)
+    encode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((__nv_bfloat16 *)u, src, L, dc, dev != nullptr);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decode(int storage, float *dst, const void *u, const Layout &L, const DevCode *dev, cudaStream_t s)
+{
+  const int g = grid_for((long long)L.n1 * L.n2 * NV, 256);
+  const DevCode dc = dev ? *dev : DevCode{};
+  if (storage == ST_F16) decode_kernel<__half><<<g, 256, 0, s>>>(dst, (const __half *)u, L, dc, dev != nullptr);
+  else if (storage == ST_BF16)
+    decode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>(dst, (const __nv_bfloat16 *)u, L, dc, dev != nullptr);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

@@ -26,6 +26,8 @@ struct StageArgs {
   Status *status;       // device status block (launch errors; per-grid blocks are in GridDesc)
   int nb = 0;           // tile height in blocks of 7 rows (0: the default)
   int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
+  double comp_bg = 0;   // beta * gamma of the next stage: 16-bit state carries its rounding
+                        // residual into that stage through v (0: no next stage)
 };
 
 enum StageKind : int {
@@ -52,12 +54,14 @@ struct GridDesc {
   double inv1, inv2;      // 1 / Delta per axis (batch launches scale by these)
   double inv11, inv22, inv12;  // 1 / (Delta1 Delta1), 1 / (Delta2 Delta2), 1 / (Delta1 Delta2)
   double delta1;          // Delta1
+  DevCode dev;            // deviation-storage codes (FP16 / BF16 arrays)
 };
 
 // Fills a GridDesc (tensor maps over u_in and v encoded here).  Returns CUDA_SUCCESS or the
 // driver's error.
 CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
-                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0);
+                        int p2, double delta1, double delta2, const double *dt, Status *status, int tile0,
+                        const DevCode *dev = nullptr);
 // Tile height of the substage kernel in blocks of 7 output rows, unless a launch sets nb.
 constexpr int TILE_BLOCKS_DEFAULT = 5;
 // Tiles of one grid for a tile height of nb blocks of 7 rows (0: the default).
@@ -79,11 +83,17 @@ cudaError_t launch_fill(int storage, void *p, size_t count, double value, cudaSt
 // max over the interior of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2, in double, as
 // an atomic max into status->smax
 cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const double *para, double delta1,
-                              double delta2, Status *status, cudaStream_t s);
+                              double delta2, Status *status, cudaStream_t s, const DevCode *dev = nullptr);
 // FP64 sums of the conserved densities, deterministic: partials[nblocks * 4] then out[4]
 int sums_blocks(const Layout &L);
 cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *partials, double *out,
-                        cudaStream_t s);
+                        cudaStream_t s, const DevCode *dev = nullptr);
+// Deviation storage: interior cells of the FP32 cell array src (n1 x n2 x NVAR, no ghosts)
+// encoded into the 16-bit array u with the codes dev; and back (dev null: v, plain 16-bit).
+cudaError_t launch_encode(int storage, void *u, const float *src, const Layout &L, const DevCode *dev,
+                          cudaStream_t s);
+cudaError_t launch_decode(int storage, float *dst, const void *u, const Layout &L, const DevCode *dev,
+                          cudaStream_t s);
 // Device-resident time step: dt <- min(courant / smax, dt_diff, t_end - t), t <- t + dt
 // (applied by the caller's order: the update runs before the step that uses dt and
 // advances t by it), smax reset to 0 for the step's last stage to refill.

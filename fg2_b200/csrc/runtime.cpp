@@ -23,6 +23,7 @@
 #include <state.h>
 #include <eqns.cuh>
 #include <Euler.cuh>
+#include <bcond.cuh>
 #include <config.h>
 #include <init.h>
 
@@ -94,8 +95,11 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p1 = s->p1;
   a.p2 = s->p2;
   a.status = s->status;
+  a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
   return a;
 }
+
+const DevCode *dev_code(const fg2_sim *s) { return s->dev_storage ? &s->dev : nullptr; }
 
 // The two ping-pong descriptors (boundaries and Delta as configured); uploaded before any
 // capture, since every path that launches a substage calls this first.
@@ -104,7 +108,7 @@ int ensure_descs(fg2_sim *s)
   if (s->desc_valid) return FG2_OK;
   for (int k = 0; k < 2; ++k)
     if (make_grid_desc(&s->desc_host[k], s->u[k], s->u[1 - k], s->v, s->L, s->storage, s->p1, s->p2, s->delta1,
-                       s->delta2, nullptr, s->status, 0) != CUDA_SUCCESS)
+                       s->delta2, nullptr, s->status, 0, dev_code(s)) != CUDA_SUCCESS)
       return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
   CK(cudaMemcpyAsync(s->desc, s->desc_host, 2 * sizeof(GridDesc), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -139,6 +143,7 @@ int do_bcond(fg2_sim *s)
 
 int do_euler(fg2_sim *s, double dt)
 {
+  if (s->dev_storage) return fail(FG2_ERR_UNSUPPORTED, "the Euler hook needs FP32 or FP64 storage");
   if (!s->fixed_phases) {  // the reference's RANDOMIZE: two phases per Euler call
     s->r1 = (float)(6.2831853071795865 * s->forcing.uniform());
     s->r2 = (float)(6.2831853071795865 * s->forcing.uniform());
@@ -199,10 +204,68 @@ int read_status(fg2_sim *s)
   return FG2_OK;
 }
 
+// Deviation storage: the codes of a host state (float, n1 x n2 x NVAR): per-field mean as
+// background (0 for fields a reflecting wall negates), per 64 x 64 tile the largest
+// deviation as scale (1 where the tile equals the background).  Uploaded to the device.
+int set_codes(fg2_sim *s, const float *x)
+{
+  const int nv = scheme::NVAR, T = SCALE_TILE;
+  for (int f = 0; f < 4; ++f) s->dev.bg[f] = 0.f;
+  for (int f = 0; f < nv; ++f) {
+    if (scheme::reflect_sign(f) < 0) continue;
+    double sum = 0.0;
+    for (size_t c = 0; c < (size_t)s->n1 * s->n2; ++c) sum += x[c * nv + f];
+    s->dev.bg[f] = (float)(sum / ((double)s->n1 * s->n2));
+  }
+  std::vector<float4> sc((size_t)s->tiles1 * s->tiles2), iv(sc.size());
+  for (int ti = 0; ti < s->tiles1; ++ti)
+    for (int tj = 0; tj < s->tiles2; ++tj) {
+      float m[4] = {0.f, 0.f, 0.f, 0.f};
+      for (int i = ti * T; i < std::min(s->n1, (ti + 1) * T); ++i)
+        for (int j = tj * T; j < std::min(s->n2, (tj + 1) * T); ++j)
+          for (int f = 0; f < nv; ++f) m[f] = std::max(m[f], std::fabs(x[((size_t)i * s->n2 + j) * nv + f] - s->dev.bg[f]));
+      for (int f = 0; f < 4; ++f)
+        if (!(m[f] > 0.f) || !std::isfinite(m[f])) m[f] = 1.f;
+      const size_t t = (size_t)ti * s->tiles2 + tj;
+      sc[t] = make_float4(m[0], m[1], m[2], m[3]);
+      iv[t] = make_float4(1.f / m[0], 1.f / m[1], 1.f / m[2], 1.f / m[3]);
+    }
+  CK(cudaMemcpyAsync(s->scale_dev, sc.data(), sc.size() * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->inv_dev, iv.data(), iv.size() * sizeof(float4), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  drop_graph(s);  // descriptors carry the background
+  return FG2_OK;
+}
+
+// Deviation storage: host float cells <-> 16-bit device array through an FP32 device copy.
+// The state u is coded with new codes on upload; v is plain 16-bit.
+int transfer_dev(fg2_sim *s, void *dev_array, void *host, bool to_device)
+{
+  const bool is_u = dev_array != s->v;
+  const size_t n = (size_t)s->n1 * s->n2 * scheme::NVAR;
+  float *tmp = nullptr;
+  CK(cudaMalloc(&tmp, n * sizeof(float)));
+  std::unique_ptr<float, cudaError_t (*)(void *)> hold(tmp, cudaFree);
+  if (to_device) {
+    if (is_u) {
+      int rc = set_codes(s, (const float *)host);
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(tmp, host, n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CK(launch_encode(s->storage, dev_array, tmp, s->L, is_u ? &s->dev : nullptr, s->stream));
+  } else {
+    CK(launch_decode(s->storage, tmp, dev_array, s->L, is_u ? &s->dev : nullptr, s->stream));
+    CK(cudaMemcpyAsync(host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  return FG2_OK;
+}
+
 // host array (rows of n2 cells x NVAR values) <-> device layout.  The device rows hold the
 // same interleaved cells as the host rows, so a transfer is one strided 2D copy.
 int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
 {
+  if (s->dev_storage) return transfer_dev(s, dev_array, host, to_device);
   const size_t elem = elem_size(s->storage);
   if (host_elem(s->storage) != elem) return fail(FG2_ERR_UNSUPPORTED, "storage %d has no host transfer", s->storage);
   const size_t hrow = (size_t)s->n2 * scheme::NVAR * elem, drow = (size_t)s->L.RS * elem;
@@ -274,12 +337,15 @@ fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_a
     fail(FG2_ERR_ARG, "grid %d x %d is smaller than the ghost width %d", n1, n2, HALF);
     return nullptr;
   }
-  if (storage != ST_F32 && storage != ST_F64) {
-    fail(FG2_ERR_UNSUPPORTED, "storage %d is not supported by the plain path", storage);
+  if (storage != ST_F32 && storage != ST_F64 && storage != ST_F16 && storage != ST_BF16) {
+    fail(FG2_ERR_UNSUPPORTED, "unknown storage %d", storage);
     return nullptr;
   }
   std::unique_ptr<fg2_sim> s(new fg2_sim);
   s->own_arrays = own_arrays;
+  s->dev_storage = storage == ST_F16 || storage == ST_BF16;
+  s->tiles1 = (n1 + SCALE_TILE - 1) / SCALE_TILE;
+  s->tiles2 = (n2 + SCALE_TILE - 1) / SCALE_TILE;
   s->n1 = n1;
   s->n2 = n2;
   s->storage = storage;
@@ -299,10 +365,25 @@ fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_a
   if (cudaMalloc(&s->sums_partial, sizeof(double) * 4 * sums_blocks(s->L)) != cudaSuccess ||
       cudaMalloc(&s->sums_out, sizeof(double) * 4) != cudaSuccess || cudaMalloc(&s->queue, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&s->desc, 3 * sizeof(GridDesc)) != cudaSuccess ||
-      cudaMemsetAsync(s->queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess) {
+      cudaMemsetAsync(s->queue, 0, 2 * sizeof(int), s->stream) != cudaSuccess ||
+      (s->dev_storage && (cudaMalloc(&s->scale_dev, sizeof(float4) * s->tiles1 * s->tiles2) != cudaSuccess ||
+                          cudaMalloc(&s->inv_dev, sizeof(float4) * s->tiles1 * s->tiles2) != cudaSuccess))) {
     fail(FG2_ERR_ALLOC, "device allocation of the handle's buffers failed");
     fg2_sim_destroy(s.release());
     return nullptr;
+  }
+  if (s->dev_storage) {
+    for (int f = 0; f < 4; ++f) s->dev.bg[f] = 0.f;
+    s->dev.scale = s->scale_dev;
+    s->dev.inv = s->inv_dev;
+    s->dev.tiles2 = s->tiles2;
+    const std::vector<float4> one((size_t)s->tiles1 * s->tiles2, make_float4(1.f, 1.f, 1.f, 1.f));
+    if (cudaMemcpy(s->scale_dev, one.data(), one.size() * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->inv_dev, one.data(), one.size() * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess) {
+      fail(FG2_ERR_ALLOC, "scale initialisation failed");
+      fg2_sim_destroy(s.release());
+      return nullptr;
+    }
   }
   return s.release();
 }
@@ -372,6 +453,8 @@ void fg2_sim_destroy(fg2_sim *s)
   cudaFree(s->sums_out);
   cudaFree(s->queue);
   cudaFree(s->desc);
+  cudaFree(s->scale_dev);
+  cudaFree(s->inv_dev);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -512,7 +595,8 @@ double fg2_sim_getdt(fg2_sim *s)
     return (double)(float)s->c / (double)den;
   }
   if (cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream) != cudaSuccess ||
-      launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream) !=
+      launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream,
+                        dev_code(s)) !=
           cudaSuccess ||
       cudaMemcpyAsync(s->status_host, s->status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess) {
@@ -546,7 +630,8 @@ int fg2_sim_advance(fg2_sim *s, int nsteps, double dt, double t_end)
   const bool device_dt = !(dt > 0);
   if (device_dt && !s->smax_valid) {
     CK(cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream));
-    CK(launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream));
+    CK(launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream,
+                         dev_code(s)));
     s->smax_valid = true;
   }
   for (int n = 0; n < nsteps; ++n) {
@@ -672,6 +757,7 @@ int fg2_sim_kick(fg2_sim *s, double t, double beta)
 int fg2_sim_drift(fg2_sim *s, double dt)
 {
   if (!s) return fail(FG2_ERR_ARG, "null handle");
+  if (s->dev_storage) return fail(FG2_ERR_UNSUPPORTED, "drift needs FP32 or FP64 storage");
   const double r = s->storage == ST_F64 ? dt : (double)(float)dt;
   CK(launch_drift(s->storage, s->u[s->cur], s->v, s->L, r, s->status, s->stream));
   s->ghosts_valid = false;
@@ -720,7 +806,7 @@ int fg2_sim_seed_forcing(fg2_sim *s, uint64_t seed)
 int fg2_sim_sums(fg2_sim *s, double out[4])
 {
   if (!s || !out) return fail(FG2_ERR_ARG, "null argument");
-  CK(launch_sums(s->storage, s->u[s->cur], s->L, s->sums_partial, s->sums_out, s->stream));
+  CK(launch_sums(s->storage, s->u[s->cur], s->L, s->sums_partial, s->sums_out, s->stream, dev_code(s)));
   CK(cudaMemcpyAsync(out, s->sums_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   return FG2_OK;

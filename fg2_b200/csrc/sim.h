@@ -52,6 +52,11 @@ struct fg2_sim {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};  // two-step graph per ping-pong parity
   double graph_dt[2] = {0, 0}, graph_tend[2] = {0, 0};
   char para_msg[256];
+  // deviation storage (FP16 / BF16 arrays): per-field background and per-tile scales
+  bool dev_storage = false;
+  int tiles1 = 0, tiles2 = 0;
+  float4 *scale_dev = nullptr, *inv_dev = nullptr;
+  fg2::DevCode dev{};
 };
 
 namespace fg2 {
@@ -75,6 +80,8 @@ int do_euler(fg2_sim *s, double dt);
 bool euler_active(const fg2_sim *s);
 double diffusive_dt(const fg2_sim *s);
 int read_status(fg2_sim *s);
+// The handle's deviation codes for kernels that decode the state (null: plain storage).
+const fg2::DevCode *dev_code(const fg2_sim *s);
 void drop_graph(fg2_sim *s);
 // A handle over caller-owned device memory: arrays u0, u1, v of the handle's layout and one
 // status block (device) with its pinned host mirror; the handle frees none of them.

@@ -36,6 +36,14 @@
 // into a max.  Register slots are indexed by row mod 7 and the row loop is unrolled by 7, so
 // the window never moves.
 //
+// Deviation storage.  With FP16 / BF16 state arrays (S = __half / __nv_bfloat16) the stencil
+// still runs in FP32: when a u chunk lands, the CTA decodes it (bg + s h, s of the cell's
+// 64 x 64 tile) into an FP32 copy in shared memory that the stencil reads; v is converted on
+// load; u' is encoded with its tile's 1/s and v stored as 16-bit numbers.  The rounding
+// residual e = encode(u') - u' of a stage that has a successor is carried into that stage
+// through v: v is stored as v - e / (beta' gamma' dt), so the next update u'' = u'(stored) +
+// gamma' dt (F + beta' v) subtracts e again (src/step.cpp:24-35 unchanged otherwise).
+//
 // Stencil weights.  A single-grid launch folds 1/Delta into the weights (constant-bank
 // operands).  A batch launch (SC) uses the reference's plain weights and multiplies each
 // derivative by its grid's 1/Delta factors, which it keeps in registers, as the reference
@@ -58,22 +66,37 @@ constexpr int NP = (NV + 1) / 2;   // field pairs
 static_assert(NT == SW, "one thread per strip column");
 static_assert(scheme::U1 == 1 && scheme::U2 == 2, "u1 and u2 are fields 1 and 2");
 
+// Cells per TMA group of a storage type: the innermost box dimension is one group of
+// interleaved cells and must be a multiple of 16 bytes.
+__host__ __device__ constexpr int group_of(int elem)
+{
+  return ((elem >= 8 ? 2 : 4) * NV * elem) % 16 == 0 ? (elem >= 8 ? 2 : 4) : 2 * (elem >= 8 ? 2 : 4);
+}
+
 // Shared memory of one CTA: NSLOT slots of [u box | v box] (the v box only when the stage
-// reads v), then the mbarriers and the producer's bookkeeping.
-template <class T, bool RV>
+// reads v), the FP32 copy of the landed u box (deviation storage), then the mbarriers and
+// the producer's bookkeeping.  The v box starts VOFF cells left of the strip when a cell
+// group is wider than the 4 ghost columns.
+template <class S, bool RV>
 struct Geo {
+  static constexpr bool DEV = Store<S>::DEV;
   static constexpr int NSLOT = FG2_NSLOT;
-  static constexpr int G = 16 / (int)sizeof(T);  // cells per 16-byte group (TMA box unit)
-  static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * NV * sizeof(T));
+  static constexpr int CB = NV * (int)sizeof(S);  // bytes per cell
+  static constexpr int G = group_of((int)sizeof(S));
+  static constexpr int VOFF = GL % G;
+  static constexpr int VBW = (SW + VOFF + G - 1) / G * G;
+  static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * CB);
   static constexpr uint32_t V_OFF = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
-  static constexpr uint32_t V_BYTES = (uint32_t)(SW * CH * NV * sizeof(T));
+  static constexpr uint32_t V_BYTES = (uint32_t)(VBW * CH * CB);
   static constexpr uint32_t SLOT = V_OFF + (RV ? (V_BYTES + 127) / 128 * 128 : 0);
-  static constexpr size_t BAR_OFF = (size_t)NSLOT * SLOT;
+  static constexpr size_t DEC_OFF = (size_t)NSLOT * SLOT;
+  static constexpr size_t DEC_BYTES = DEV ? (size_t)BW * CH * NV * sizeof(float) : 0;
+  static constexpr size_t BAR_OFF = DEC_OFF + (DEC_BYTES + 127) / 128 * 128;
   // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
   static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
-  static_assert(BW % G == 0 && SW % G == 0 && GL % G == 0, "boxes and tile origins are whole cell groups");
-  static_assert(BW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
+  static_assert(BW % G == 0 && VBW % G == 0 && (GL - VOFF) % G == 0, "boxes and tile origins are whole cell groups");
+  static_assert(BW / G <= 256 && VBW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
 };
 
 // One cell's NV values as field pairs ((lnd, u1), (u2, lne)): one or two 16-byte accesses for
@@ -112,6 +135,82 @@ __device__ __forceinline__ void st_cell(T *p, const typename PairOf<T>::type in[
   }
 }
 
+// One cell of a storage array as compute-type field pairs, and back (16-bit storage converts).
+template <class S>
+__device__ __forceinline__ void load_cell(const S *p, typename PairOf<typename Store<S>::C>::type out[NP])
+{
+  using St = Store<S>;
+  if constexpr (!St::DEV) {
+    ld_cell<S>(p, out);
+  } else if constexpr (NV == 4) {
+    const uint2 w = *reinterpret_cast<const uint2 *>(p);
+    out[0] = St::to2(*reinterpret_cast<const typename St::S2 *>(&w.x));
+    out[1] = St::to2(*reinterpret_cast<const typename St::S2 *>(&w.y));
+  } else {
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+      out[q] = make_float2(St::to(p[2 * q]), 2 * q + 1 < NV ? St::to(p[2 * q + 1]) : 0.f);
+  }
+}
+
+template <class S>
+__device__ __forceinline__ void store_cell(S *p, const typename PairOf<typename Store<S>::C>::type in[NP])
+{
+  using St = Store<S>;
+  if constexpr (!St::DEV) {
+    st_cell<S>(p, in);
+  } else if constexpr (NV == 4) {
+    const typename St::S2 a = St::from2(in[0]), b = St::from2(in[1]);
+    uint2 w;
+    w.x = *reinterpret_cast<const unsigned *>(&a);
+    w.y = *reinterpret_cast<const unsigned *>(&b);
+    *reinterpret_cast<uint2 *>(p) = w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      p[2 * q] = St::from(in[q].x);
+      if (2 * q + 1 < NV) p[2 * q + 1] = St::from(in[q].y);
+    }
+  }
+}
+
+// Deviation storage: stores the 16-bit numbers of h (field pairs) at p and returns them as
+// stored (raw) and converted back (hs).
+template <class S>
+__device__ __forceinline__ void encode_cell(S *p, const float2 h[NP], float2 hs[NP], S raw[NV])
+{
+  using St = Store<S>;
+  if constexpr (NV == 4) {
+    const typename St::S2 a = St::from2(h[0]), b = St::from2(h[1]);
+    uint2 w;
+    w.x = *reinterpret_cast<const unsigned *>(&a);
+    w.y = *reinterpret_cast<const unsigned *>(&b);
+    *reinterpret_cast<uint2 *>(p) = w;
+    hs[0] = St::to2(a);
+    hs[1] = St::to2(b);
+    raw[0] = a.x;
+    raw[1] = a.y;
+    raw[2] = b.x;
+    raw[3] = b.y;
+  } else {
+#pragma unroll
+    for (int f = 0; f < NV; ++f) {
+      raw[f] = St::from((f & 1) ? h[f >> 1].y : h[f >> 1].x);
+      p[f] = raw[f];
+    }
+#pragma unroll
+    for (int q = 0; q < NP; ++q) hs[q] = make_float2(St::to(raw[2 * q]), 2 * q + 1 < NV ? St::to(raw[2 * q + 1]) : 0.f);
+  }
+}
+
+// Interior cell whose value a padded index i (ghost or padding) holds, clamped into the grid.
+__device__ __forceinline__ int source_index(int i, int n, int periodic)
+{
+  if (i < 0) i = periodic ? i + n : -1 - i;
+  else if (i >= n) i = periodic ? i - n : 2 * n - 1 - i;
+  return min(max(i, 0), n - 1);
+}
+
 // Tiles of one grid: strip fastest, so horizontally adjacent tiles run together and share
 // their halo columns through L2.
 struct TileGrid {
@@ -146,16 +245,22 @@ struct Roll {
 };
 
 // Everything a thread needs of the grid its current tile belongs to (registers).
-template <class T>
+template <class S>
 struct GridRegs {
+  using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
   Layout L;
-  T *u_out, *v;
+  S *u_out, *v;
   Status *status;
   int p1, p2;
   P gdt;                       // gamma dt of this grid's step, both lanes
   P s1, s2, s11, s22;          // 1/Delta factors (batch launches)
   T s12, inv1, inv2, delta1;   // 1/(Delta1 Delta2), CFL factors, Delta1
+  // deviation storage
+  P bg[NP];                    // per-field background
+  P comp;                      // 1 / (beta' gamma' dt) of the next stage, or 0
+  const float4 *scale, *inv;   // per-tile s and 1/s
+  int tiles2;
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
@@ -219,9 +324,8 @@ __device__ __forceinline__ void lead_row(const T *su, int tx, const KParams<T> &
 }
 
 // Derivatives of field pair PI at the output row held in register slot S0, into a Cell.
-template <class T, unsigned M2, bool SC, int S0, int PI>
-__device__ __forceinline__ void emit_pair(const KParams<T> &a, const GridRegs<T> &gr, const Roll<T> &s,
-                                          Cell<T, NV> &cell)
+template <class T, unsigned M2, bool SC, int S0, int PI, class GR>
+__device__ __forceinline__ void emit_pair(const KParams<T> &a, const GR &gr, const Roll<T> &s, Cell<T, NV> &cell)
 {
   using P = typename PairOf<T>::type;
   const P c = s.w[PI][S0];
@@ -267,11 +371,14 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const GridRegs<T>
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
 // vr is v of the cell (read stages).  u' and v go straight to HBM; edge cells also write
 // their ghost images.
-template <class T, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], int i, int j, const KParams<T> &a,
-                                         const GridRegs<T> &gr, const Roll<T> &s, bool &nan, T &rate)
+template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
+__device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
+                                         const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
+                                         const Roll<typename Store<S>::C> &s, bool &nan, typename Store<S>::C &rate)
 {
+  using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
+  using St = Store<S>;
   constexpr int S0 = (R + 4) % CH;
   Cell<T, NV> cell;
   emit_pair<T, M2, SC, S0, 0>(a, gr, s, cell);
@@ -292,15 +399,45 @@ __device__ __forceinline__ void emit_row(const typename PairOf<T>::type vr[NP], 
     qp[p] = fmac(gr.gdt, vn[p], s.w[p][S0]);
   }
   const long long o = gr.L.at(0, i, j);
-  if (WRITE_U) st_cell<T>(gr.u_out + o, qp);
-  if (WRITE_V) st_cell<T>(gr.v + o, vn);
+  if constexpr (!St::DEV) {
+    if (WRITE_U) store_cell<S>(gr.u_out + o, qp);
+    if (WRITE_V) store_cell<S>(gr.v + o, vn);
+  }
+  S raw[NV];
+  if constexpr (St::DEV) {
+    if (WRITE_U) {
+      // encode u' with its tile's 1/s; the residual of the rounding goes into v
+      const int t = (i / SCALE_TILE) * gr.tiles2 + j / SCALE_TILE;
+      const float4 iv = __ldg(gr.inv + t);
+      const P ivp[2] = {make_float2(iv.x, iv.y), make_float2(iv.z, iv.w)};
+      P h[NP], hs[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) h[p] = (qp[p] - gr.bg[p]) * ivp[p];
+      encode_cell<S>(gr.u_out + o, h, hs, raw);
+      if (WRITE_V) {
+        const float4 sc = __ldg(gr.scale + t);
+        const P scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
+#pragma unroll
+        for (int p = 0; p < NP; ++p) vn[p] = vn[p] - (fmac(scp[p], hs[p], gr.bg[p]) - qp[p]) * gr.comp;
+      }
+    }
+  }
+  if constexpr (St::DEV) {
+    if (WRITE_V) store_cell<S>(gr.v + o, vn);
+  }
   if (WRITE_U) {
     T qn[NV];
 #pragma unroll
     for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
 #pragma unroll
     for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
-    store_ghosts<T, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
+    if constexpr (!St::DEV) {
+      store_ghosts<S, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
+    } else {
+      // images carry the stored numbers, negated where the wall flips the sign
+      const bool edge = i < HALF || i >= gr.L.n1 - HALF || j < HALF || j >= gr.L.n2 - HALF;
+      if (edge) store_ghosts<S, S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
+    }
     if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2));
   }
 }
@@ -328,12 +465,12 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 }
 
 // Issues the next chunk of the CTA's sequence into its slot (free by the caller's check).
-template <class T, bool READ_V>
+template <class S, bool READ_V>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
                                             int *queue)
 {
-  using G = Geo<T, READ_V>;
+  using G = Geo<S, READ_V>;
   if (ps->done) return;
   const int n = ps->next_n, s = n % G::NSLOT;
   if (ps->c == 0) {
@@ -363,7 +500,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     tma_load_3d(smem + (size_t)s * G::SLOT, &gd.tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
     // v of the 7 output rows of block c - 1
     if (with_v)
-      tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL) / G::G,
+      tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
                   i0 + CH * (c - 1) + GT);
     ps->c = c == nb ? 0 : c + 1;
   }
@@ -371,18 +508,21 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
 }
 
 // Loads the registers of grid g (every thread; the loads are uniform across the CTA).
-template <class T, bool SC>
-__device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<T> &a, GridRegs<T> &gr)
+template <class S, bool SC>
+__device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<typename Store<S>::C> &a,
+                                          GridRegs<S> &gr)
 {
+  using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
   gr.L = gd.L;
-  gr.u_out = reinterpret_cast<T *>(gd.u_out);
-  gr.v = reinterpret_cast<T *>(gd.v);
+  gr.u_out = reinterpret_cast<S *>(gd.u_out);
+  gr.v = reinterpret_cast<S *>(gd.v);
   gr.status = gd.status;
   gr.p1 = gd.p1;
   gr.p2 = gd.p2;
+  const double dt = gd.dt ? *gd.dt : a.dt_dev ? *a.dt_dev : a.dt;
   // (R)(dt * gamma[i]), src/step.cpp:34
-  gr.gdt = lit<P>(a.gamma * (gd.dt ? *gd.dt : a.dt_dev ? *a.dt_dev : a.dt));
+  gr.gdt = lit<P>(a.gamma * dt);
   if (SC) {
     gr.s1 = lit<P>(gd.inv1);
     gr.s2 = lit<P>(gd.inv2);
@@ -395,6 +535,37 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<T> &
   } else {
     gr.inv1 = a.ks.inv1;
     gr.inv2 = a.ks.inv2;
+  }
+  if constexpr (Store<S>::DEV) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) gr.bg[p] = make_float2(gd.dev.bg[2 * p], gd.dev.bg[2 * p + 1]);
+    gr.comp = lit<P>(a.comp_bg != 0.0 && dt > 0.0 ? 1.0 / (a.comp_bg * dt) : 0.0);
+    gr.scale = gd.dev.scale;
+    gr.inv = gd.dev.inv;
+    gr.tiles2 = gd.dev.tiles2;
+  }
+}
+
+// Deviation storage: the landed 7-row u box (padded rows prow0 .., padded columns from j0)
+// decoded into FP32 cells, bg + s h with s of the tile of the interior cell each value
+// images.  Thread tx decodes box columns tx and tx + 128.
+template <class S>
+__device__ __forceinline__ void decode_chunk(const S *box, float *dec, int prow0, int j0, const GridRegs<S> &gr)
+{
+  const int n1 = gr.L.n1, n2 = gr.L.n2;
+  for (int cc = threadIdx.x; cc < BW; cc += NT) {
+    const int tj = source_index(j0 - GL + cc, n2, gr.p2) / SCALE_TILE;
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      const int ti = source_index(prow0 + r - GT, n1, gr.p1) / SCALE_TILE;
+      const float4 sc = __ldg(gr.scale + ti * gr.tiles2 + tj);
+      const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
+      float2 h[NP];
+      load_cell<S>(box + (r * BW + cc) * NV, h);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
+      st_cell<float>(dec + (r * BW + cc) * NV, h);
+    }
   }
 }
 
@@ -416,12 +587,14 @@ __device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
   rate = T(0);
 }
 
-template <class T, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
+template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
-                                                         const KParams<T> a, int *queue)
+                                                         const KParams<typename Store<S>::C> a, int *queue)
 {
+  using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
-  using G = Geo<T, READ_V>;
+  using G = Geo<S, READ_V>;
+  constexpr bool DEV = Store<S>::DEV;
   constexpr int NS = G::NSLOT;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
@@ -437,14 +610,14 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
+    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
   }
   __syncthreads();
 
   bool nan = false;
   T rate = T(0);
   const int tx = threadIdx.x;  // column within the strip
-  GridRegs<T> gr;
+  GridRegs<S> gr;
   int cur_g = -1;
   Roll<T> st;
   int n = 0;  // chunks consumed
@@ -458,14 +631,15 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
       break;
     }
-    const T *su = reinterpret_cast<const T *>(smem + (size_t)s * G::SLOT);
+    const S *sbox = reinterpret_cast<const S *>(smem + (size_t)s * G::SLOT);
+    const T *su = reinterpret_cast<const T *>(smem + (DEV ? G::DEC_OFF : (size_t)s * G::SLOT));
     if (b < 0) {
       const int tile = tile_of[s];
       if (tile < 0) break;
       const int g = grid_of[s];
       if (g != cur_g) {
         if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);
-        load_grid<T, SC>(grids[g], a, gr);
+        load_grid<S, SC>(grids[g], a, gr);
         cur_g = g;
       }
       const int local = tile - grids[g].tile0, strips = grids[g].strips;
@@ -475,6 +649,10 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       for (int g2 = 0; g2 < 2; ++g2)
 #pragma unroll
         for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
+      if constexpr (DEV) {
+        decode_chunk<S>(sbox, reinterpret_cast<float *>(smem + G::DEC_OFF), i0 - 4 + GT, j0, gr);
+        __syncthreads();
+      }
       // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
       lead_row<T, M2, 0>(su, tx, a, st);
       lead_row<T, M2, 1>(su, tx, a, st);
@@ -485,20 +663,24 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       lead_row<T, M2, 6>(su, tx, a, st);
     } else {
       const int ib = i0 + CH * b, j = j0 + tx;
-      const T *sv = su + G::V_OFF / sizeof(T);
+      const S *sv = sbox + G::V_OFF / sizeof(S);
+      if constexpr (DEV) {
+        decode_chunk<S>(sbox, reinterpret_cast<float *>(smem + G::DEC_OFF), ib + 3 + GT, j0, gr);
+        __syncthreads();
+      }
 #define FG2_ROW(R)                                                                                \
   {                                                                                               \
     P vrow[NP];                                                                                   \
-    if (READ_V) ld_cell<T>(sv + (R * SW + tx) * NV, vrow);                                        \
+    if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
     lead_row<T, M2, R>(su, tx, a, st);                                                            \
-    emit_row<T, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
   }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<T, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
+      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }
