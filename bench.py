@@ -401,7 +401,9 @@ def run_fused(args):
     device = torch.device("cuda", local)
     dist = dist_init(world, "nccl")
 
-    sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage="f32")
+    sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=args.storage)
+    elem = 2 if args.storage in ("f16", "bf16") else 4
+    b_alg = B_ALG * elem // ELEM  # 160 B per cell-step in FP32, 80 B with 16-bit storage
     sim.config()
     state = initial_state()
     sim.upload(state)
@@ -446,8 +448,8 @@ def run_fused(args):
     if sim.sync() != 0:
         raise RuntimeError("stage timing produced a bad status")
     peak, peak_kind = peaks()
-    achieved = B_ALG * cells / (sum(stage_ms) / 1e3) / 1e9  # GB/s over the three launches
-    traffic = profiled_traffic("substage_hydro_f32_4096")
+    achieved = b_alg * cells / (sum(stage_ms) / 1e3) / 1e9  # GB/s over the three launches
+    traffic = profiled_traffic(f"substage_hydro_{args.storage}_4096")
 
     # end to end through the public API: pinned host state in, K steps, state out
     e2e, e2e_status = None, None
@@ -455,11 +457,11 @@ def run_fused(args):
         e2e, e2e_status = run_e2e(sim, state, stream, args, dist, device, world, cells)
 
     batch = None
-    if rank == 0 and world == 1 and not args.no_batch:
+    if rank == 0 and world == 1 and not args.no_batch and args.storage == "f32":
         batch = run_batch_leg(200, args.warmup, device)
 
     mixed, precision = None, None
-    if rank == 0 and world == 1 and not args.no_mixed:
+    if rank == 0 and world == 1 and not args.no_mixed and args.storage == "f32":
         mixed = run_mixed_leg(state, args.steps, args.warmup, device, value / world)
         precision = run_precision_leg(8192, 500, device)
 
@@ -474,9 +476,10 @@ def run_fused(args):
         line = {
             "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32",
+            "vs_baseline": None, "dtype": "f32" if args.storage == "f32" else f"{args.storage} storage, f32 math",
             "data": "synthetic: seeded tanh Kelvin-Helmholtz shear layer (setup kh, seed 2)",
-            "config": {"workload": WORKLOAD, "scheme": SCHEME, "grid": [N1, N2], "setup": SETUP, "seed": SEED,
+            "config": {"workload": WORKLOAD if args.storage == "f32" else WORKLOAD.replace("plain FP32", f"{args.storage} deviation storage"),
+                       "storage": args.storage, "scheme": SCHEME, "grid": [N1, N2], "setup": SETUP, "seed": SEED,
                        "dt": "CFL + diffusive limit, FP64, device-resident", "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (u, u' and v are 268 MB each)"},
             "ns_per_cell_step": 1.0 / (value / world),
@@ -484,8 +487,8 @@ def run_fused(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "frac_nominal_8tbs": achieved / 8000.0,
-                         "bytes_per_cell_step": B_ALG, "stage_ms": stage_ms},
-            "step_hbm_frac": value / world * B_ALG / peak,
+                         "bytes_per_cell_step": b_alg, "stage_ms": stage_ms},
+            "step_hbm_frac": value / world * b_alg / peak,
             "cpu_baseline": cpu,
             "e2e": e2e, "e2e_status": e2e_status,
             "batch": batch,
@@ -510,6 +513,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch (secondary) leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 16-bit storage and precision legs")
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
+                    help="state storage of the headline workload (f16/bf16: deviation storage)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -55,12 +55,18 @@ namespace sub {
 #ifndef FG2_NSLOT
 #define FG2_NSLOT 2
 #endif
+#ifndef FG2_WARP_PIPE
+#define FG2_WARP_PIPE 0
+#endif
+#ifndef FG2_SW
+#define FG2_SW 128
+#endif
 
-constexpr int SW = 128;            // interior columns per tile (strip width)
+constexpr int SW = FG2_SW;         // interior columns per tile (strip width)
 constexpr int BW = SW + 2 * GL;    // TMA box width of u (halo 4 + 4; the stencil uses 3)
 constexpr int CH = 7;              // rows per chunk = register window period
 constexpr int NB_DEFAULT = TILE_BLOCKS_DEFAULT;  // output blocks per tile unless a launch sets nb
-constexpr int NCW = 4;             // warps per CTA
+constexpr int NCW = SW / 32;       // warps per CTA
 constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
 constexpr int NP = (NV + 1) / 2;   // field pairs
 static_assert(NT == SW, "one thread per strip column");
@@ -90,10 +96,13 @@ struct Geo {
   static constexpr uint32_t V_BYTES = (uint32_t)(VBW * CH * CB);
   static constexpr uint32_t SLOT = V_OFF + (RV ? (V_BYTES + 127) / 128 * 128 : 0);
   static constexpr size_t DEC_OFF = (size_t)NSLOT * SLOT;
-  static constexpr size_t DEC_BYTES = DEV ? (size_t)BW * CH * NV * sizeof(float) : 0;
+  static constexpr int DW = 32 + 6;  // columns of a warp's decoded copy (its 32 columns and the halo)
+  static constexpr size_t DEC_BYTES =
+      DEV ? (FG2_WARP_PIPE ? (size_t)NCW * CH * DW * NV * sizeof(float) : (size_t)BW * CH * NV * sizeof(float)) : 0;
   static constexpr size_t BAR_OFF = DEC_OFF + (DEC_BYTES + 127) / 128 * 128;
-  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
-  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
+  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], done[NSLOT], abort flag,
+  // producer state
+  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 3 * NSLOT * sizeof(int) + 12 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
   static_assert(BW % G == 0 && VBW % G == 0 && (GL - VOFF) % G == 0, "boxes and tile origins are whole cell groups");
   static_assert(BW / G <= 256 && VBW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
@@ -294,12 +303,12 @@ __device__ __forceinline__ void lead_pair(const typename PairOf<T>::type (&x)[7]
 }
 
 // Leading-row work for register slot R: loads the 7 cells of row R of the chunk around the
-// thread's column.
-template <class T, unsigned M2, int R>
-__device__ __forceinline__ void lead_row(const T *su, int tx, const KParams<T> &a, Roll<T> &s)
+// thread's column; base points at column j-3 of row 0, rows are RSTRIDE elements apart.
+template <class T, unsigned M2, int R, int RSTRIDE>
+__device__ __forceinline__ void lead_row(const T *base, const KParams<T> &a, Roll<T> &s)
 {
   using P = typename PairOf<T>::type;
-  const T *row = su + (R * BW + tx + GL - 3) * NV;
+  const T *row = base + R * RSTRIDE;
   P x[7][NP];
 #pragma unroll
   for (int k = 0; k < 7; ++k) ld_cell<T>(row + k * NV, x[k]);
@@ -546,14 +555,17 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
   }
 }
 
-// Deviation storage: the landed 7-row u box (padded rows prow0 .., padded columns from j0)
-// decoded into FP32 cells, bg + s h with s of the tile of the interior cell each value
-// images.  Thread tx decodes box columns tx and tx + 128.
+// Deviation storage: decodes box columns c0 .. c0 + ncol of the landed 7-row u box (padded
+// rows prow0 .., box column 0 = padded column j0) into FP32 cells dec ([row][ncol][NV]):
+// bg + s h with s of the tile of the interior cell each value images.  This thread takes
+// every step-th column from `first`.
 template <class S>
-__device__ __forceinline__ void decode_chunk(const S *box, float *dec, int prow0, int j0, const GridRegs<S> &gr)
+__device__ __forceinline__ void decode_cols(const S *box, float *dec, int ncol, int c0, int first, int step, int prow0,
+                                            int j0, const GridRegs<S> &gr)
 {
   const int n1 = gr.L.n1, n2 = gr.L.n2;
-  for (int cc = threadIdx.x; cc < BW; cc += NT) {
+  for (int c = first; c < ncol; c += step) {
+    const int cc = c0 + c;
     const int tj = source_index(j0 - GL + cc, n2, gr.p2) / SCALE_TILE;
 #pragma unroll
     for (int r = 0; r < CH; ++r) {
@@ -564,7 +576,7 @@ __device__ __forceinline__ void decode_chunk(const S *box, float *dec, int prow0
       load_cell<S>(box + (r * BW + cc) * NV, h);
 #pragma unroll
       for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
-      st_cell<float>(dec + (r * BW + cc) * NV, h);
+      st_cell<float>(dec + (r * ncol + c) * NV, h);
     }
   }
 }
@@ -596,14 +608,21 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   using G = Geo<S, READ_V>;
   constexpr bool DEV = Store<S>::DEV;
   constexpr int NS = G::NSLOT;
+  constexpr bool WP = FG2_WARP_PIPE != 0;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
   int *tile_of = reinterpret_cast<int *>(full + NS);
   int *grid_of = tile_of + NS;
-  Producer *ps = reinterpret_cast<Producer *>(grid_of + NS);
+  int *done = grid_of + NS;            // warps finished with the chunk in each slot
+  volatile int *abort = done + NS;     // a warp gave up waiting
+  Producer *ps = reinterpret_cast<Producer *>(done + NS + 4);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      done[s] = 0;
+    }
+    *abort = 0;
     fence_mbar_init();
     ps->next_n = 0;
     ps->tile = -1;
@@ -617,22 +636,45 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   bool nan = false;
   T rate = T(0);
   const int tx = threadIdx.x;  // column within the strip
+  const int warp = tx >> 5, lane = tx & 31;
   GridRegs<S> gr;
   int cur_g = -1;
   Roll<T> st;
   int n = 0;  // chunks consumed
   int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
+  // the stencil's source: the landed box, or (16-bit storage) the decoded copy, whole-CTA or
+  // this warp's 38 columns
+  float *decw = reinterpret_cast<float *>(smem + G::DEC_OFF) + (WP ? (size_t)warp * CH * G::DW * NV : 0);
+  constexpr int RSTRIDE = DEV ? (WP ? G::DW * NV : BW * NV) : BW * NV;
 
   for (;;) {
     const int s = n % NS;
-    // the chunk has landed (every thread waits, the CTA agrees)
-    const bool landed = mbar_wait_bounded(&full[s], (uint32_t)((n / NS) & 1), WAIT_NS);
-    if (__syncthreads_or(!landed)) {
-      if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-      break;
+    const uint32_t parity = (uint32_t)((n / NS) & 1);
+    if constexpr (WP) {
+      // each warp waits for the chunk on its own; a warp that gives up raises the abort flag,
+      // and the others stop at their next wait
+      bool landed = *abort == 0 && mbar_wait_bounded(&full[s], parity, WAIT_NS);
+      landed = __all_sync(0xffffffffu, landed);
+      if (!landed) {
+        if (lane == 0) {
+          *abort = 1;
+          atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
+        }
+        break;
+      }
+    } else {
+      // the chunk has landed (every thread waits, the CTA agrees)
+      const bool landed = mbar_wait_bounded(&full[s], parity, WAIT_NS);
+      if (__syncthreads_or(!landed)) {
+        if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
+        break;
+      }
     }
     const S *sbox = reinterpret_cast<const S *>(smem + (size_t)s * G::SLOT);
-    const T *su = reinterpret_cast<const T *>(smem + (DEV ? G::DEC_OFF : (size_t)s * G::SLOT));
+    const T *base;
+    if constexpr (DEV) base = reinterpret_cast<const T *>(decw) + (WP ? lane : tx + GL - 3) * NV;
+    else base = reinterpret_cast<const T *>(sbox) + (tx + GL - 3) * NV;
+    int prow0;  // padded row of the box's first row
     if (b < 0) {
       const int tile = tile_of[s];
       if (tile < 0) break;
@@ -645,42 +687,63 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       const int local = tile - grids[g].tile0, strips = grids[g].strips;
       i0 = (local / strips) * (a.nb * CH);
       j0 = (local % strips) * SW;
+      prow0 = i0 - 4 + GT;
+    } else {
+      prow0 = i0 + CH * b + 3 + GT;
+    }
+    if constexpr (DEV) {
+      if constexpr (WP) {
+        // this warp's columns j0 + 32 warp - 3 .. + 34: box columns 32 warp + 1 ..
+        decode_cols<S>(sbox, decw, G::DW, 32 * warp + GL - 3, lane, 32, prow0, j0, gr);
+        __syncwarp();
+      } else {
+        decode_cols<S>(sbox, decw, BW, 0, tx, NT, prow0, j0, gr);
+        __syncthreads();
+      }
+    }
+    if (b < 0) {
 #pragma unroll
       for (int g2 = 0; g2 < 2; ++g2)
 #pragma unroll
         for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
-      if constexpr (DEV) {
-        decode_chunk<S>(sbox, reinterpret_cast<float *>(smem + G::DEC_OFF), i0 - 4 + GT, j0, gr);
-        __syncthreads();
-      }
       // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
-      lead_row<T, M2, 0>(su, tx, a, st);
-      lead_row<T, M2, 1>(su, tx, a, st);
-      lead_row<T, M2, 2>(su, tx, a, st);
-      lead_row<T, M2, 3>(su, tx, a, st);
-      lead_row<T, M2, 4>(su, tx, a, st);
-      lead_row<T, M2, 5>(su, tx, a, st);
-      lead_row<T, M2, 6>(su, tx, a, st);
+      lead_row<T, M2, 0, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 1, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 2, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 3, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 4, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 5, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 6, RSTRIDE>(base, a, st);
     } else {
       const int ib = i0 + CH * b, j = j0 + tx;
       const S *sv = sbox + G::V_OFF / sizeof(S);
-      if constexpr (DEV) {
-        decode_chunk<S>(sbox, reinterpret_cast<float *>(smem + G::DEC_OFF), ib + 3 + GT, j0, gr);
-        __syncthreads();
-      }
 #define FG2_ROW(R)                                                                                \
   {                                                                                               \
     P vrow[NP];                                                                                   \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
-    lead_row<T, M2, R>(su, tx, a, st);                                                            \
+    lead_row<T, M2, R, RSTRIDE>(base, a, st);                                                     \
     emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
   }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
     }
-    __syncthreads();  // everyone is done with slot s
-    if (threadIdx.x == 0)
-      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
+    if constexpr (WP) {
+      // release slot s: the last warp done with it issues the next chunk into it
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence_block();
+        if (atomicAdd(&done[s], 1) == NCW - 1) {
+          __threadfence_block();  // the previous producer's state and every warp's release
+          done[s] = 0;
+          issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
+        }
+      }
+      __syncwarp();
+    } else {
+      __syncthreads();  // everyone is done with slot s
+      if (threadIdx.x == 0)
+        issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
+    }
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }
