@@ -392,6 +392,99 @@ def run_precision_leg(n, steps, device):
     return result
 
 
+# ---- batch + 16-bit storage (secondary result) ----------------------------------------------
+COMBINED_SIDES = (512, 1024, 2048)
+COMBINED_COUNT, COMBINED_SEED, COMBINED_STEPS = 64, 5, 300
+
+
+def run_combined_leg(device):
+    """64 hydro sims (sides from {512, 1024, 2048} by seed 5, k^-2 random-phase velocity at rms
+    Mach 0.5, rho = 1, p = 1/gamma): the FP16 batch against the same sims advanced one at a
+    time in plain FP32 (and, for reference, as an FP32 batch), all with one fixed dt (0.9 x the
+    smallest member CFL step) for 300 steps, replayed from graphs; errors against an FP64
+    batch with the same steps."""
+    import torch
+    import fg2_b200
+    rng = np.random.default_rng(COMBINED_SEED)
+    sizes = [(int(x), int(x)) for x in rng.choice(COMBINED_SIDES, size=COMBINED_COUNT)]
+    states = [fg2_b200.setup_evaluate("turb", n1, n2, SCHEME, seed=COMBINED_SEED * 1000 + k)[0]
+              for k, (n1, n2) in enumerate(sizes)]
+    cells = sum(n1 * n2 for n1, n2 in sizes)
+
+    def timed(fn, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # the common step: 0.9 x the FP64 CFL step of the finest member (the smallest over members)
+    k_fine = max(range(len(sizes)), key=lambda k: sizes[k][0])
+    with fg2_b200.Sim(*sizes[k_fine], scheme=SCHEME, storage="f64") as s:
+        s.config()
+        s.upload(states[k_fine])
+        s.set_dt_mode("cfl")
+        dt = 0.9 * s.getdt()
+
+    def run_batch(storage, time_it):
+        b = fg2_b200.Batch(sizes, scheme=SCHEME, storage=storage)
+        b.config()
+        for k, m in enumerate(b.members):
+            m.upload(states[k] if storage == "f64" else states[k].astype(np.float32))
+        stream = torch.cuda.ExternalStream(b.stream, device=device)
+        if time_it:
+            b.autotune(reps=2)
+        b.advance(2, dt, graph=True)  # warm-up: captures the graph ...
+        for k, m in enumerate(b.members):  # ... then back to the initial states
+            m.upload(states[k] if storage == "f64" else states[k].astype(np.float32))
+        ms = timed(lambda: b.advance(COMBINED_STEPS, dt, graph=True), stream)
+        status = b.sync()
+        outs = [m.download() for m in b.members]
+        b.close()
+        return ms, status, outs
+
+    ms64, st64, ref = run_batch("f64", False)
+    ms16, st16, out16 = run_batch("f16", True)
+    msb32, stb32, outb32 = run_batch("f32", True)
+    # the plain FP32 path, one simulation after another on one stream
+    stream = torch.cuda.Stream(device=device)
+    sims = []
+    for k, (n1, n2) in enumerate(sizes):
+        s = fg2_b200.Sim(n1, n2, scheme=SCHEME, storage="f32", stream=stream.cuda_stream)
+        s.config()
+        s.upload(states[k].astype(np.float32))
+        s.advance(2, dt, graph=True)
+        s.upload(states[k].astype(np.float32))
+        sims.append(s)
+    ms32 = timed(lambda: [s.advance(COMBINED_STEPS, dt, graph=True) for s in sims], stream)
+    st32 = max(s.sync() for s in sims)
+    out32 = [s.download() for s in sims]
+    for s in sims:
+        s.close()
+
+    def rho_err(outs):
+        num = sum(((np.exp(o[..., 0].astype(np.float64)) - np.exp(r[..., 0])) ** 2).sum() for o, r in zip(outs, ref))
+        den = sum((np.exp(r[..., 0]) ** 2).sum() for r in ref)
+        return float(np.sqrt(num / den))
+
+    v16 = cells * COMBINED_STEPS / (ms16 / 1e3) / 1e9
+    v32 = cells * COMBINED_STEPS / (ms32 / 1e3) / 1e9
+    vb32 = cells * COMBINED_STEPS / (msb32 / 1e3) / 1e9
+    e16, e32, eb32 = rho_err(out16), rho_err(out32), rho_err(outb32)
+    return {"workload": f"{len(sizes)} hydro sims, sides {list(COMBINED_SIDES)} drawn with seed {COMBINED_SEED}, "
+                        f"k^-2 random-phase velocity rms Mach 0.5, fixed dt {dt:.4g}, {COMBINED_STEPS} steps",
+            "cells": cells, "dt": dt,
+            "f16_batch": {"value": v16, "unit": "Gcell-steps/s", "ms_per_step": ms16 / COMBINED_STEPS, "status": st16,
+                          "rho_rel_l2_vs_f64": e16},
+            "f32_one_at_a_time": {"value": v32, "unit": "Gcell-steps/s", "ms_per_step": ms32 / COMBINED_STEPS,
+                                  "status": st32, "rho_rel_l2_vs_f64": e32},
+            "f32_batch": {"value": vb32, "unit": "Gcell-steps/s", "ms_per_step": msb32 / COMBINED_STEPS,
+                          "status": stb32, "rho_rel_l2_vs_f64": eb32},
+            "speedup": v16 / v32, "error_ratio": e16 / max(e32, 1e-300), "f64_status": st64}
+
+
 def run_fused(args):
     import torch
     import fg2_b200
@@ -460,10 +553,11 @@ def run_fused(args):
     if rank == 0 and world == 1 and not args.no_batch and args.storage == "f32":
         batch = run_batch_leg(200, args.warmup, device)
 
-    mixed, precision = None, None
+    mixed, precision, combined = None, None, None
     if rank == 0 and world == 1 and not args.no_mixed and args.storage == "f32":
         mixed = run_mixed_leg(state, args.steps, args.warmup, device, value / world)
         precision = run_precision_leg(8192, 500, device)
+        combined = run_combined_leg(device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -494,6 +588,7 @@ def run_fused(args):
             "batch": batch,
             "mixed": mixed,
             "precision": precision,
+            "combined": combined,
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }

@@ -55,9 +55,6 @@ namespace sub {
 #ifndef FG2_NSLOT
 #define FG2_NSLOT 2
 #endif
-#ifndef FG2_WARP_PIPE
-#define FG2_WARP_PIPE 0
-#endif
 #ifndef FG2_SW
 #define FG2_SW 128
 #endif
@@ -96,13 +93,10 @@ struct Geo {
   static constexpr uint32_t V_BYTES = (uint32_t)(VBW * CH * CB);
   static constexpr uint32_t SLOT = V_OFF + (RV ? (V_BYTES + 127) / 128 * 128 : 0);
   static constexpr size_t DEC_OFF = (size_t)NSLOT * SLOT;
-  static constexpr int DW = 32 + 6;  // columns of a warp's decoded copy (its 32 columns and the halo)
-  static constexpr size_t DEC_BYTES =
-      DEV ? (FG2_WARP_PIPE ? (size_t)NCW * CH * DW * NV * sizeof(float) : (size_t)BW * CH * NV * sizeof(float)) : 0;
+  static constexpr size_t DEC_BYTES = DEV ? (size_t)BW * CH * NV * sizeof(float) : 0;
   static constexpr size_t BAR_OFF = DEC_OFF + (DEC_BYTES + 127) / 128 * 128;
-  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], done[NSLOT], abort flag,
-  // producer state
-  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 3 * NSLOT * sizeof(int) + 12 * sizeof(int) + 64;
+  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
+  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
   static_assert(BW % G == 0 && VBW % G == 0 && (GL - VOFF) % G == 0, "boxes and tile origins are whole cell groups");
   static_assert(BW / G <= 256 && VBW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
@@ -608,21 +602,14 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   using G = Geo<S, READ_V>;
   constexpr bool DEV = Store<S>::DEV;
   constexpr int NS = G::NSLOT;
-  constexpr bool WP = FG2_WARP_PIPE != 0;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
   int *tile_of = reinterpret_cast<int *>(full + NS);
   int *grid_of = tile_of + NS;
-  int *done = grid_of + NS;            // warps finished with the chunk in each slot
-  volatile int *abort = done + NS;     // a warp gave up waiting
-  Producer *ps = reinterpret_cast<Producer *>(done + NS + 4);
+  Producer *ps = reinterpret_cast<Producer *>(grid_of + NS);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NS; ++s) {
-      mbar_init(&full[s], 1);
-      done[s] = 0;
-    }
-    *abort = 0;
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
     ps->next_n = 0;
     ps->tile = -1;
@@ -636,44 +623,26 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   bool nan = false;
   T rate = T(0);
   const int tx = threadIdx.x;  // column within the strip
-  const int warp = tx >> 5, lane = tx & 31;
   GridRegs<S> gr;
   int cur_g = -1;
   Roll<T> st;
   int n = 0;  // chunks consumed
   int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
-  // the stencil's source: the landed box, or (16-bit storage) the decoded copy, whole-CTA or
-  // this warp's 38 columns
-  float *decw = reinterpret_cast<float *>(smem + G::DEC_OFF) + (WP ? (size_t)warp * CH * G::DW * NV : 0);
-  constexpr int RSTRIDE = DEV ? (WP ? G::DW * NV : BW * NV) : BW * NV;
+  // the stencil's source: the landed box, or (16-bit storage) its decoded copy
+  float *dec = reinterpret_cast<float *>(smem + G::DEC_OFF);
 
   for (;;) {
     const int s = n % NS;
     const uint32_t parity = (uint32_t)((n / NS) & 1);
-    if constexpr (WP) {
-      // each warp waits for the chunk on its own; a warp that gives up raises the abort flag,
-      // and the others stop at their next wait
-      bool landed = *abort == 0 && mbar_wait_bounded(&full[s], parity, WAIT_NS);
-      landed = __all_sync(0xffffffffu, landed);
-      if (!landed) {
-        if (lane == 0) {
-          *abort = 1;
-          atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-        }
-        break;
-      }
-    } else {
-      // the chunk has landed (every thread waits, the CTA agrees)
-      const bool landed = mbar_wait_bounded(&full[s], parity, WAIT_NS);
-      if (__syncthreads_or(!landed)) {
-        if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-        break;
-      }
+    // the chunk has landed (every thread waits, the CTA agrees)
+    const bool landed = mbar_wait_bounded(&full[s], parity, WAIT_NS);
+    if (__syncthreads_or(!landed)) {
+      if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
+      break;
     }
     const S *sbox = reinterpret_cast<const S *>(smem + (size_t)s * G::SLOT);
-    const T *base;
-    if constexpr (DEV) base = reinterpret_cast<const T *>(decw) + (WP ? lane : tx + GL - 3) * NV;
-    else base = reinterpret_cast<const T *>(sbox) + (tx + GL - 3) * NV;
+    // column j - 3 of the box's row 0
+    const T *base = (DEV ? reinterpret_cast<const T *>(dec) : reinterpret_cast<const T *>(sbox)) + (tx + GL - 3) * NV;
     int prow0;  // padded row of the box's first row
     if (b < 0) {
       const int tile = tile_of[s];
@@ -692,14 +661,8 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       prow0 = i0 + CH * b + 3 + GT;
     }
     if constexpr (DEV) {
-      if constexpr (WP) {
-        // this warp's columns j0 + 32 warp - 3 .. + 34: box columns 32 warp + 1 ..
-        decode_cols<S>(sbox, decw, G::DW, 32 * warp + GL - 3, lane, 32, prow0, j0, gr);
-        __syncwarp();
-      } else {
-        decode_cols<S>(sbox, decw, BW, 0, tx, NT, prow0, j0, gr);
-        __syncthreads();
-      }
+      decode_cols<S>(sbox, dec, BW, 0, tx, NT, prow0, j0, gr);
+      __syncthreads();
     }
     if (b < 0) {
 #pragma unroll
@@ -707,13 +670,13 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
 #pragma unroll
         for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
       // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
-      lead_row<T, M2, 0, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 1, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 2, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 3, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 4, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 5, RSTRIDE>(base, a, st);
-      lead_row<T, M2, 6, RSTRIDE>(base, a, st);
+      lead_row<T, M2, 0, BW * NV>(base, a, st);
+      lead_row<T, M2, 1, BW * NV>(base, a, st);
+      lead_row<T, M2, 2, BW * NV>(base, a, st);
+      lead_row<T, M2, 3, BW * NV>(base, a, st);
+      lead_row<T, M2, 4, BW * NV>(base, a, st);
+      lead_row<T, M2, 5, BW * NV>(base, a, st);
+      lead_row<T, M2, 6, BW * NV>(base, a, st);
     } else {
       const int ib = i0 + CH * b, j = j0 + tx;
       const S *sv = sbox + G::V_OFF / sizeof(S);
@@ -721,29 +684,15 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   {                                                                                               \
     P vrow[NP];                                                                                   \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
-    lead_row<T, M2, R, RSTRIDE>(base, a, st);                                                     \
+    lead_row<T, M2, R, BW * NV>(base, a, st);                                                     \
     emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
   }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
     }
-    if constexpr (WP) {
-      // release slot s: the last warp done with it issues the next chunk into it
-      __syncwarp();
-      if (lane == 0) {
-        __threadfence_block();
-        if (atomicAdd(&done[s], 1) == NCW - 1) {
-          __threadfence_block();  // the previous producer's state and every warp's release
-          done[s] = 0;
-          issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
-        }
-      }
-      __syncwarp();
-    } else {
-      __syncthreads();  // everyone is done with slot s
-      if (threadIdx.x == 0)
-        issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
-    }
+    __syncthreads();  // everyone is done with slot s
+    if (threadIdx.x == 0)
+      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }
