@@ -377,7 +377,8 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const GR &gr, con
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
-                                         const Roll<typename Store<S>::C> &s, bool &nan, typename Store<S>::C &rate)
+                                         const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
+                                         typename Store<S>::C &rate)
 {
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
@@ -393,7 +394,7 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
 
   T r[NV];
   scheme::eqns<M2>(cell, a.p, i, j, r, SC ? gr.delta1 : a.ks.delta1);
-  if (i >= gr.L.n1 || j >= gr.L.n2) return;  // cells past the grid
+  if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
   P vn[NP], qp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
@@ -432,14 +433,19 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
     T qn[NV];
 #pragma unroll
     for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
+    // one NaN test per cell: a NaN in any field makes the sum NaN
+    T sum = qn[0];
 #pragma unroll
-    for (int f = 0; f < NV; ++f) nan |= qn[f] != qn[f];
-    if constexpr (!St::DEV) {
-      store_ghosts<S, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
-    } else {
-      // images carry the stored numbers, negated where the wall flips the sign
-      const bool edge = i < HALF || i >= gr.L.n1 - HALF || j < HALF || j >= gr.L.n2 - HALF;
-      if (edge) store_ghosts<S, S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
+    for (int f = 1; f < NV; ++f) sum += qn[f];
+    nan |= sum != sum;
+    if (rim) {  // tiles within HALF cells of an edge
+      if constexpr (!St::DEV) {
+        store_ghosts<S, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
+      } else {
+        // images carry the stored numbers, negated where the wall flips the sign
+        const bool edge = i < HALF || i >= gr.L.n1 - HALF || j < HALF || j >= gr.L.n2 - HALF;
+        if (edge) store_ghosts<S, S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
+      }
     }
     if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2));
   }
@@ -558,12 +564,15 @@ __device__ __forceinline__ void decode_cols(const S *box, float *dec, int ncol, 
                                             int j0, const GridRegs<S> &gr)
 {
   const int n1 = gr.L.n1, n2 = gr.L.n2;
+  const int i0 = prow0 - GT;
+  const bool rows_inside = i0 >= 0 && i0 + CH <= n1;  // no ghost row in the box
   for (int c = first; c < ncol; c += step) {
+    const int j = j0 - GL + c0 + c;
     const int cc = c0 + c;
-    const int tj = source_index(j0 - GL + cc, n2, gr.p2) / SCALE_TILE;
+    const int tj = (j >= 0 && j < n2 ? j : source_index(j, n2, gr.p2)) / SCALE_TILE;
 #pragma unroll
     for (int r = 0; r < CH; ++r) {
-      const int ti = source_index(prow0 + r - GT, n1, gr.p1) / SCALE_TILE;
+      const int ti = (rows_inside ? i0 + r : source_index(i0 + r, n1, gr.p1)) / SCALE_TILE;
       const float4 sc = __ldg(gr.scale + ti * gr.tiles2 + tj);
       const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
       float2 h[NP];
@@ -628,6 +637,7 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
   Roll<T> st;
   int n = 0;  // chunks consumed
   int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
+  bool whole = false, rim = true;  // the tile lies inside the grid / within HALF cells of an edge
   // the stencil's source: the landed box, or (16-bit storage) its decoded copy
   float *dec = reinterpret_cast<float *>(smem + G::DEC_OFF);
 
@@ -657,6 +667,9 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
       i0 = (local / strips) * (a.nb * CH);
       j0 = (local % strips) * SW;
       prow0 = i0 - 4 + GT;
+      const int th = a.nb * CH;
+      whole = i0 + th <= gr.L.n1 && j0 + SW <= gr.L.n2;
+      rim = i0 < HALF || i0 + th > gr.L.n1 - HALF || j0 < HALF || j0 + SW > gr.L.n2 - HALF;
     } else {
       prow0 = i0 + CH * b + 3 + GT;
     }
@@ -685,7 +698,7 @@ __global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restr
     P vrow[NP];                                                                                   \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
     lead_row<T, M2, R, BW * NV>(base, a, st);                                                     \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, nan, rate); \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, whole, rim, nan, rate); \
   }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
