@@ -100,6 +100,34 @@ def test_port_parity_seeded(scheme, n1, n2, cuda):
     assert np.all(err <= 1e-5), err
 
 
+def test_small_plain_configuration_100_steps(cuda):
+    """The small plain configuration in full: hydro 256^2 periodic, rho = 1, p = 1/gamma, Gaussian
+    velocity noise (sigma 0.01, seed 1), the reference's dt = c / (n1/l1 + n2/l2) with c = 0.5,
+    100 steps, against the reference's arithmetic on the CPU (the port, FP32) and against the
+    FP64 port: the GPU's FP32 error against FP64 stays within 3x the CPU port's own FP32 error."""
+    n1 = n2 = 256
+    with fg2_b200.Sim(n1, n2) as sim:
+        sim.config()
+        sim.init("noise", seed=1)
+        x0 = sim.download()
+        dt = sim.getdt()
+        assert dt == reference_dt(n1, n2, 1.0, 1.0)
+        for n in range(100):
+            assert sim.step(n * dt, dt) == 0
+        gpu = sim.download()
+    outs = {}
+    for prec in ("f32", "f64"):
+        o = Oracle("hydro", prec, "port")
+        o.set_delta(*reference_delta(n1, n2, 1.0, 1.0) if prec == "f32" else (1.0 / n1, 1.0 / n2))
+        u = o.padded(x0.astype(o.dtype))
+        v = o.empty(n1, n2)
+        assert o.run(u, v, 0.0, dt, 100) == 0
+        outs[prec] = o.interior(u).astype(np.float64)
+    assert np.all(rel_l2(gpu, outs["f32"]) <= 1e-5), rel_l2(gpu, outs["f32"])
+    err_gpu, err_cpu = rel_l2(gpu, outs["f64"]), rel_l2(outs["f32"], outs["f64"])
+    assert np.all(err_gpu <= np.maximum(3 * err_cpu, 1e-7)), (err_gpu, err_cpu)
+
+
 def test_fused_step_equals_reference_building_blocks(cuda):
     """step() == Euler + 3 x (bcond, kick, drift) through the separate entry points."""
     n1, n2 = 48, 40
