@@ -247,7 +247,7 @@ def batch_sizes(count=BATCH_COUNT, seed=BATCH_SEED):
     return [(int(x), int(x)) for x in rng.choice(BATCH_SIDES, size=count)]
 
 
-def run_batch_leg(steps, warmup, device):
+def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
     """512 independent hydro-isot simulations (sides 64..512, box 2 pi, random-phase k^-2
     velocity at rms Mach 0.3): one persistent launch per substage over every member's tiles,
     two-step CUDA graph, per-member device-resident CFL steps, autotuned tiling.  Beside it,
@@ -263,7 +263,11 @@ def run_batch_leg(steps, warmup, device):
     for k, m in enumerate(b.members):
         m.init("turb", seed=BATCH_SEED * 100000 + k)
     x0 = [m.download() for m in b.members]
-    tune_ms = b.autotune(reps=4)
+    if tiling:
+        b.set_tiling(*tiling)
+        tune_ms = None
+    else:
+        tune_ms = b.autotune(reps=4)
     nb, ctas = b.tiling()
     cells = b.cells
     stream = torch.cuda.ExternalStream(b.stream, device=device)
@@ -282,6 +286,17 @@ def run_batch_leg(steps, warmup, device):
     value = cells * steps / (ms / 1e3) / 1e9
     peak, _ = peaks()
     b.close()
+
+    result = {"workload": f"{len(sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
+                          "box 2 pi, k^-2 random-phase velocity rms Mach 0.3, FP32, per-member CFL dt",
+              "cells": cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
+              "status": status, "tiling": {"blocks_of_7_rows": nb, "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
+              "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
+                           "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
+                           "frac": value * B_ALG_ISOT / peak},
+              "gpu_launches_per_step": 4}
+    if not one_at_a_time:
+        return result
 
     # the same simulations one at a time through the single-grid path, on one stream
     k_alone = min(steps, 20)
@@ -305,17 +320,10 @@ def run_batch_leg(steps, warmup, device):
     for s in sims:
         s.close()
     alone = cells * k_alone / (ms_alone / 1e3) / 1e9
-    return {"workload": f"{len(sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
-                        "box 2 pi, k^-2 random-phase velocity rms Mach 0.3, FP32, per-member CFL dt",
-            "cells": cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
-            "status": status, "tiling": {"blocks_of_7_rows": nb, "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
-            "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
-                         "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
-                         "frac": value * B_ALG_ISOT / peak},
-            "one_at_a_time": {"value": alone, "steps": k_alone, "ms_per_step": ms_alone / k_alone,
-                              "what": "same members, single-grid path, one simulation after another"},
-            "speedup_vs_one_at_a_time": value / alone,
-            "gpu_launches_per_step": 4}
+    result["one_at_a_time"] = {"value": alone, "steps": k_alone, "ms_per_step": ms_alone / k_alone,
+                               "what": "same members, single-grid path, one simulation after another"}
+    result["speedup_vs_one_at_a_time"] = value / alone
+    return result
 
 
 # ---- the 16-bit deviation-storage path (secondary results) ----------------------------------
@@ -489,6 +497,12 @@ def run_fused(args):
     import torch
     import fg2_b200
 
+    if args.only_batch:  # the batch leg alone (profiling): fixed tiling, no one-at-a-time leg
+        torch.cuda.set_device(0)
+        tiling = tuple(int(x) for x in args.batch_tiling.split(",")) if args.batch_tiling else None
+        print(json.dumps(run_batch_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling, False)), flush=True)
+        return
+
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
@@ -608,6 +622,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch (secondary) leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 16-bit storage and precision legs")
+    ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
+    ap.add_argument("--batch-tiling", default="", help="nb,ctas_per_sm for the batch leg (default: autotune)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
                     help="state storage of the headline workload (f16/bf16: deviation storage)")
     args = ap.parse_args()

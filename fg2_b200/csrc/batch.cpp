@@ -469,8 +469,9 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
     double ms;
   };
   std::vector<Cand> cands;
+  // CTAs per SM: 0 = as many as fit (the occupancy limit), or capped at 1, 2 or 3
   for (int nb : {2, 3, 4, 5, 6, 8})
-    for (int ctas = 1; ctas <= 3; ++ctas) cands.push_back({nb, ctas, std::numeric_limits<double>::infinity()});
+    for (int ctas : {0, 1, 2, 3}) cands.push_back({nb, ctas, std::numeric_limits<double>::infinity()});
   const int keep_nb = b->nb, keep_ctas = b->max_ctas;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));

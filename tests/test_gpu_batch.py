@@ -161,7 +161,7 @@ def test_autotune_keeps_state(cuda):
         ms = b.autotune(reps=2)
         assert ms > 0
         nb, ctas = b.tiling()
-        assert 2 <= nb <= 8 and 1 <= ctas <= 3
+        assert 2 <= nb <= 8 and 0 <= ctas <= 3
         for a, m in zip(before, b.members):
             assert np.array_equal(a, m.download())
         assert b.advance(2, 1e-3) == 0 and b.sync() == 0
