@@ -438,12 +438,47 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
 #pragma unroll
     for (int f = 1; f < NV; ++f) sum += qn[f];
     nan |= sum != sum;
-    if (rim) {  // tiles within HALF cells of an edge
-      if constexpr (!St::DEV) {
+    if (rim) {  // tiles within HALF cells of an edge: the cell's ghost images for the next stage
+      const int n1 = gr.L.n1, n2 = gr.L.n2;
+      if (n1 >= 2 * HALF && n2 >= 2 * HALF) {
+        // at most one row image and one column image (and their corner), stored whole; column
+        // images across a wall negate the fields the scheme reflects (16-bit storage: those
+        // fields have bg = 0, so the stored number is negated)
+        int ia = -(1 << 30), ja = -(1 << 30);
+        if (i < HALF) ia = gr.p1 ? i + n1 : -1 - i;
+        else if (i >= n1 - HALF) ia = gr.p1 ? i - n1 : 2 * n1 - 1 - i;
+        if (j < HALF) ja = gr.p2 ? j + n2 : -1 - j;
+        else if (j >= n2 - HALF) ja = gr.p2 ? j - n2 : 2 * n2 - 1 - j;
+        if (ia > -(1 << 30) || ja > -(1 << 30)) {
+          auto put = [&](long long off, bool flip) {
+            if constexpr (!St::DEV) {
+              P w[NP];
+#pragma unroll
+              for (int p = 0; p < NP; ++p) w[p] = qp[p];
+#pragma unroll
+              for (int f = 0; f < NV; ++f)
+                if (flip && scheme::reflect_sign(f) < 0) {
+                  if (f & 1) w[f >> 1].y = -w[f >> 1].y;
+                  else w[f >> 1].x = -w[f >> 1].x;
+                }
+              store_cell<S>(gr.u_out + off, w);
+            } else {
+#pragma unroll
+              for (int f = 0; f < NV; ++f)
+                gr.u_out[off + f] = (flip && scheme::reflect_sign(f) < 0) ? -raw[f] : raw[f];
+            }
+          };
+          const bool flip = !gr.p2;
+          if (ia > -(1 << 30)) put(gr.L.at(0, ia, j), false);
+          if (ja > -(1 << 30)) {
+            put(gr.L.at(0, i, ja), flip);
+            if (ia > -(1 << 30)) put(gr.L.at(0, ia, ja), flip);
+          }
+        }
+      } else if constexpr (!St::DEV) {  // grids narrower than two ghost widths
         store_ghosts<S, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
       } else {
-        // images carry the stored numbers, negated where the wall flips the sign
-        const bool edge = i < HALF || i >= gr.L.n1 - HALF || j < HALF || j >= gr.L.n2 - HALF;
+        const bool edge = i < HALF || i >= n1 - HALF || j < HALF || j >= n2 - HALF;
         if (edge) store_ghosts<S, S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
       }
     }
