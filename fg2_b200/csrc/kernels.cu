@@ -175,9 +175,11 @@ __device__ __forceinline__ Images ghost_images(int i, int j, int n1, int n2, int
   return g;
 }
 
-// Only the ghost images of (i, j), not the cell itself (which the caller stores).
+// Only the ghost images of (i, j), not the cell itself (which the caller stores): the general
+// case, any grid size.  Kept out of line: the fused kernel calls it only for grids narrower
+// than two ghost widths, and inlined copies would crowd its instruction cache.
 template <class T, class C>
-__device__ __forceinline__ void store_ghosts(T *u, const Layout &L, int i, int j, const C q[NV], int p1, int p2)
+__device__ __noinline__ void store_ghosts(T *u, const Layout L, int i, int j, const C *q, int p1, int p2)
 {
   const bool edge = i < HALF || i >= L.n1 - HALF || j < HALF || j >= L.n2 - HALF;
   if (!edge) return;

@@ -371,6 +371,73 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const GR &gr, con
   }
 }
 
+// Ghost images of interior cell (i, j) for the next stage (the reference's bcond result,
+// src/bcond.cu:22-86): at most one row image and one column image, and their corner, each
+// stored whole; column images across a wall negate the fields the scheme reflects.  Grids
+// narrower than two ghost widths take the general path.  Out of line: only cells of tiles
+// near an edge call it, and one copy keeps the unrolled row loop small.
+template <class S>
+__device__ __noinline__ void rim_images(S *u, const Layout L, int i, int j, typename PairOf<typename Store<S>::C>::type q0,
+                                        typename PairOf<typename Store<S>::C>::type q1, int p1, int p2)
+{
+  using T = typename Store<S>::C;
+  using P = typename PairOf<T>::type;
+  const P qp[2] = {q0, q1};
+  const int n1 = L.n1, n2 = L.n2;
+  if (n1 < 2 * HALF || n2 < 2 * HALF) {
+    T qn[NV];
+#pragma unroll
+    for (int f = 0; f < NV; ++f) qn[f] = (f & 1) ? qp[f >> 1].y : qp[f >> 1].x;
+    store_ghosts<S, T>(u, L, i, j, qn, p1, p2);
+    return;
+  }
+  int ia = -(1 << 30), ja = -(1 << 30);
+  if (i < HALF) ia = p1 ? i + n1 : -1 - i;
+  else if (i >= n1 - HALF) ia = p1 ? i - n1 : 2 * n1 - 1 - i;
+  if (j < HALF) ja = p2 ? j + n2 : -1 - j;
+  else if (j >= n2 - HALF) ja = p2 ? j - n2 : 2 * n2 - 1 - j;
+  P f[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) f[p] = qp[p];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    if (!p2 && scheme::reflect_sign(k) < 0) {
+      if (k & 1) f[k >> 1].y = -f[k >> 1].y;
+      else f[k >> 1].x = -f[k >> 1].x;
+    }
+  if (ia > -(1 << 30)) store_cell<S>(u + L.at(0, ia, j), qp);
+  if (ja > -(1 << 30)) {
+    store_cell<S>(u + L.at(0, i, ja), f);
+    if (ia > -(1 << 30)) store_cell<S>(u + L.at(0, ia, ja), f);
+  }
+}
+
+// The same for 16-bit storage, with the stored numbers (reflected fields have bg = 0, so their
+// images are the negated numbers).
+template <class S>
+__device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, const S *raw, int p1, int p2)
+{
+  const int n1 = L.n1, n2 = L.n2;
+  if (n1 < 2 * HALF || n2 < 2 * HALF) {
+    store_ghosts<S, S>(u, L, i, j, raw, p1, p2);
+    return;
+  }
+  int ia = -(1 << 30), ja = -(1 << 30);
+  if (i < HALF) ia = p1 ? i + n1 : -1 - i;
+  else if (i >= n1 - HALF) ia = p1 ? i - n1 : 2 * n1 - 1 - i;
+  if (j < HALF) ja = p2 ? j + n2 : -1 - j;
+  else if (j >= n2 - HALF) ja = p2 ? j - n2 : 2 * n2 - 1 - j;
+  auto put = [&](long long off, bool flip) {
+#pragma unroll
+    for (int f = 0; f < NV; ++f) u[off + f] = (flip && scheme::reflect_sign(f) < 0) ? -raw[f] : raw[f];
+  };
+  if (ia > -(1 << 30)) put(L.at(0, ia, j), false);
+  if (ja > -(1 << 30)) {
+    put(L.at(0, i, ja), !p2);
+    if (ia > -(1 << 30)) put(L.at(0, ia, ja), !p2);
+  }
+}
+
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
 // vr is v of the cell (read stages).  u' and v go straight to HBM; edge cells also write
 // their ghost images.
@@ -439,48 +506,8 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
     for (int f = 1; f < NV; ++f) sum += qn[f];
     nan |= sum != sum;
     if (rim) {  // tiles within HALF cells of an edge: the cell's ghost images for the next stage
-      const int n1 = gr.L.n1, n2 = gr.L.n2;
-      if (n1 >= 2 * HALF && n2 >= 2 * HALF) {
-        // at most one row image and one column image (and their corner), stored whole; column
-        // images across a wall negate the fields the scheme reflects (16-bit storage: those
-        // fields have bg = 0, so the stored number is negated)
-        int ia = -(1 << 30), ja = -(1 << 30);
-        if (i < HALF) ia = gr.p1 ? i + n1 : -1 - i;
-        else if (i >= n1 - HALF) ia = gr.p1 ? i - n1 : 2 * n1 - 1 - i;
-        if (j < HALF) ja = gr.p2 ? j + n2 : -1 - j;
-        else if (j >= n2 - HALF) ja = gr.p2 ? j - n2 : 2 * n2 - 1 - j;
-        if (ia > -(1 << 30) || ja > -(1 << 30)) {
-          auto put = [&](long long off, bool flip) {
-            if constexpr (!St::DEV) {
-              P w[NP];
-#pragma unroll
-              for (int p = 0; p < NP; ++p) w[p] = qp[p];
-#pragma unroll
-              for (int f = 0; f < NV; ++f)
-                if (flip && scheme::reflect_sign(f) < 0) {
-                  if (f & 1) w[f >> 1].y = -w[f >> 1].y;
-                  else w[f >> 1].x = -w[f >> 1].x;
-                }
-              store_cell<S>(gr.u_out + off, w);
-            } else {
-#pragma unroll
-              for (int f = 0; f < NV; ++f)
-                gr.u_out[off + f] = (flip && scheme::reflect_sign(f) < 0) ? -raw[f] : raw[f];
-            }
-          };
-          const bool flip = !gr.p2;
-          if (ia > -(1 << 30)) put(gr.L.at(0, ia, j), false);
-          if (ja > -(1 << 30)) {
-            put(gr.L.at(0, i, ja), flip);
-            if (ia > -(1 << 30)) put(gr.L.at(0, ia, ja), flip);
-          }
-        }
-      } else if constexpr (!St::DEV) {  // grids narrower than two ghost widths
-        store_ghosts<S, T>(gr.u_out, gr.L, i, j, qn, gr.p1, gr.p2);
-      } else {
-        const bool edge = i < HALF || i >= n1 - HALF || j < HALF || j >= n2 - HALF;
-        if (edge) store_ghosts<S, S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
-      }
+      if constexpr (!St::DEV) rim_images<S>(gr.u_out, gr.L, i, j, qp[0], qp[NP - 1], gr.p1, gr.p2);
+      else rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
     }
     if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2));
   }
