@@ -665,7 +665,7 @@ __device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
 }
 
 template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__global__ void __launch_bounds__(NT, 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
+__global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
                                                          const KParams<typename Store<S>::C> a, int *queue)
 {
   using T = typename Store<S>::C;
