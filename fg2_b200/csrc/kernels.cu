@@ -195,25 +195,6 @@ __device__ __noinline__ void store_ghosts(T *u, const Layout L, int i, int j, co
     }
 }
 
-template <class T, class C>
-__device__ __forceinline__ void store_images(T *u, const Layout &L, int i, int j, const C q[NV], int p1, int p2)
-{
-  const bool edge = i < HALF || i >= L.n1 - HALF || j < HALF || j >= L.n2 - HALF;
-  if (!edge) {
-#pragma unroll
-    for (int f = 0; f < NV; ++f) u[L.at(f, i, j)] = (T)q[f];
-    return;
-  }
-  const Images g = ghost_images(i, j, L.n1, L.n2, p1, p2);
-  for (int a = 0; a < g.nr; ++a)
-    for (int b = 0; b < g.nc; ++b)
-#pragma unroll
-      for (int f = 0; f < NV; ++f) {
-        const C x = (g.flip[b] && scheme::reflect_sign(f) < 0) ? -q[f] : q[f];
-        u[L.at(f, g.rows[a], g.cols[b])] = (T)x;
-      }
-}
-
 template <class C>
 __device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2)
 {

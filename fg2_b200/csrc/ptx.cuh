@@ -22,13 +22,6 @@ __device__ __forceinline__ void fence_mbar_init()
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Order this thread's generic-proxy shared-memory accesses before later async-proxy ones
-// (needed before a TMA load overwrites a buffer the threads just read).
-__device__ __forceinline__ void fence_proxy_async_smem()
-{
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
 {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -74,35 +67,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
       "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
-}
-
-// 3D tiled TMA store of one box from shared memory (bulk async-group completion).  The
-// caller fences its shared-memory writes to the async proxy first.
-__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y, int z)
-{
-  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map), "r"(x),
-               "r"(y), "r"(z), "r"(smem_u32(src))
-               : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-
-// Wait until the bulk groups this thread committed have finished reading shared memory.
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-
-// Wait until the bulk groups this thread committed have completed.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-// Prefetch one box of a tensor into L2 (no shared memory, no completion tracking).
-__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z)
-{
-  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(x), "r"(y), "r"(z)
-               : "memory");
-}
-
-__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map)
-{
-  asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
 
 }  // namespace fg2
