@@ -55,6 +55,7 @@ struct fg2_batch {
   std::vector<int> curs;
   // tiling (autotuned or set)
   int nb = TILE_BLOCKS_DEFAULT, max_ctas = 0;
+  int reverse = 0;  // tile order of the next substage launch (alternates)
   // the two-step graph and what it was captured for
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0, graph_tend = 0;
@@ -136,6 +137,8 @@ int enqueue_batch_step(fg2_batch *b, double dt, bool device_dt, double t_end, in
     a.status = b->status;
     a.nb = b->nb;
     a.max_ctas = b->max_ctas;
+    a.reverse = b->reverse;
+    b->reverse ^= 1;
     a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
     CK(launch_substage(b->storage, kind, device_dt && k == 2, true, b->desc + (size_t)set * b->count, b->count,

@@ -91,6 +91,7 @@ struct KParams {
   const double *dt_dev;  // device time step for grids without their own, or null: dt
   Status *status;        // launch errors
   int nb;                // output blocks of 7 rows per tile
+  int reverse;           // tiles last first
   double comp_bg;        // beta * gamma of the next stage (16-bit residual carry), or 0
 };
 
@@ -147,6 +148,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.status = a.status;
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
   kp.comp_bg = a.comp_bg;
+  kp.reverse = a.reverse;
   return kp;
 }
 

@@ -28,6 +28,8 @@ struct StageArgs {
   int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
   double comp_bg = 0;   // beta * gamma of the next stage: 16-bit state carries its rounding
                         // residual into that stage through v (0: no next stage)
+  int reverse = 0;      // take the tiles last first (alternated from launch to launch, so a
+                        // stage starts on the tiles the previous one wrote last, still in L2)
 };
 
 enum StageKind : int {

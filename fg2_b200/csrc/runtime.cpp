@@ -119,7 +119,10 @@ int ensure_descs(fg2_sim *s)
 // One substage of the state u[cur] into u[1 - cur] (kick: v only).
 int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridDesc *desc)
 {
-  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L), a, s->queue, s->stream));
+  StageArgs b = a;
+  b.reverse = s->order;
+  s->order ^= 1;
+  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L), b, s->queue, s->stream));
   return FG2_OK;
 }
 

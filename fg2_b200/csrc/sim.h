@@ -32,6 +32,7 @@ struct fg2_sim {
   fg2::GridDesc desc_host[3];
   bool desc_valid = false;
   unsigned version = 0;       // bumped whenever settings that descriptors depend on change
+  int order = 0;              // tile order of the next substage launch (alternates)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
   bool own_stream = false;

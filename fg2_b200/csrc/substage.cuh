@@ -539,7 +539,7 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 template <class S, bool READ_V>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
-                                            int *queue)
+                                            bool reverse, int *queue)
 {
   using G = Geo<S, READ_V>;
   if (ps->done) return;
@@ -547,6 +547,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
   if (ps->c == 0) {
     int t = atomicAdd(&queue[0], 1);
     if (t >= ntiles) t = -1;
+    else if (reverse) t = ntiles - 1 - t;
     ps->tile = t;
     tile_of[s] = t;
     if (t >= 0) {
@@ -687,7 +688,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1)
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);
+    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, queue);
   }
   __syncthreads();
 
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1)
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, queue);  // refill slot s
+      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, queue);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }
