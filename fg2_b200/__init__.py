@@ -66,6 +66,7 @@ def _bind(lib):
         "fg2_drift": (None, [P, P, ctypes.c_float]), "fg2_bcond": (None, [P, I, I]),
         "fg2_Euler": (None, [P, ctypes.c_float]), "fg2_global": (P, []),
         "fg2_sums_noalloc": (I, [P, I, I, LL, I, P, P]),
+        "fg2_sim_solve": (I, [P, D, D, I, I, S, ctypes.POINTER(D)]),
         "fg2_batch_create": (P, [I, P, P, I, P]), "fg2_batch_destroy": (None, [P]),
         "fg2_batch_count": (I, [P]), "fg2_batch_cells": (LL, [P]), "fg2_batch_device_bytes": (SZ, [P]),
         "fg2_batch_stream": (P, [P]), "fg2_batch_member": (P, [P, I]),
@@ -275,6 +276,14 @@ class Sim:
     # ---- frames -------------------------------------------------------------------
     def dump(self, path, time):
         self._check(self.lib.fg2_sim_dump(self.h, str(path).encode(), float(time)), "dump")
+
+    def solve(self, t, t_final, i, n, directory):
+        """The reference's frame loop: frames i+1 .. n up to t_final, dumped as
+        directory/%04d.raw.  Returns (status, ms per step)."""
+        ms = ctypes.c_double()
+        rc = self.lib.fg2_sim_solve(self.h, float(t), float(t_final), int(i), int(n), str(directory).encode(),
+                                    ctypes.byref(ms))
+        return self._check(rc, "solve"), ms.value
 
     def load(self, path):
         t = ctypes.c_double()

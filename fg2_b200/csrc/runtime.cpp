@@ -893,6 +893,70 @@ int fg2_sim_load(fg2_sim *s, const char *path, double *time)
   return fg2_sim_upload(s, data.data());
 }
 
+// The reference's solve() loop (src/solve.cpp:25-64): frames i+1 .. n evenly spaced up to
+// t_final; each frame steps until its time (the last step shortened to land on it) and is
+// dumped as <dir>/<frame, 4 digits>.raw (src/misc.cpp:57-62).  The time step is the
+// handle's getdt mode: FG2_DT_REFERENCE takes getdt() on the host; FG2_DT_CFL keeps it on the
+// device (graph replay, CFL rate folded into the last substage).  A NaN dumps the state as
+// <dir>/****.raw and returns FG2_ERR_NAN, as the reference does before it aborts.
+int fg2_sim_solve(fg2_sim *s, double t, double t_final, int i, int n, const char *dir, double *ms_per_step)
+{
+  if (!s || !dir || n <= i || !(t_final > t)) return fail(FG2_ERR_ARG, "bad solve arguments");
+  ensure_config(s);
+  auto path = [&](const char *leaf) { return std::string(dir) + "/" + leaf; };
+  char leaf[64];
+  cudaEvent_t c0 = nullptr, c1 = nullptr;
+  CK(cudaEventCreate(&c0));
+  CK(cudaEventCreate(&c1));
+  std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> h0(c0, cudaEventDestroy), h1(c1, cudaEventDestroy);
+  long long total_steps = 0;
+  float total_ms = 0.f;
+  const double dt_dump = (t_final - t) / (n - i);
+  int rc = FG2_OK;
+  if ((rc = fg2_sim_set_time(s, t)) != FG2_OK) return rc;
+  while (i++ < n) {
+    const double target = t_final - (n - i) * dt_dump;
+    long long m = 0;
+    CK(cudaEventRecord(c0, s->stream));
+    if (s->dt_mode == FG2_DT_REFERENCE) {
+      while (t < target) {
+        const double dt = std::min(target - t, fg2_sim_getdt(s));
+        if ((rc = fg2_sim_step(s, t, dt)) != FG2_OK) break;
+        t = std::min(t + dt, target);
+        ++m;
+      }
+    } else {
+      // device-resident steps: the dt update caps the last step at the frame's time; chunks of
+      // steps are sized from the last step until the device clock reaches the target
+      while (rc == FG2_OK && t < target) {
+        const double last = fg2_sim_last_dt(s);
+        long long k = last > 0 ? (long long)std::ceil((target - t) / last) : 16;
+        k = std::max(1LL, std::min(k, 4096LL));
+        rc = fg2_sim_advance_graph(s, (int)k, 0.0, target);
+        if (rc == FG2_OK) rc = fg2_sim_sync(s);
+        t = fg2_sim_time(s);
+        m += k;
+        if (t >= target * (1.0 - 1e-15)) t = target;
+      }
+    }
+    CK(cudaEventRecord(c1, s->stream));
+    CK(cudaEventSynchronize(c1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c0, c1));
+    total_ms += ms;
+    total_steps += m;
+    if (rc != FG2_OK) {
+      fg2_sim_clear_status(s);
+      fg2_sim_dump(s, path("****.raw").c_str(), t);
+      break;
+    }
+    snprintf(leaf, sizeof(leaf), "%04d.raw", i);
+    if ((rc = fg2_sim_dump(s, path(leaf).c_str(), t)) != FG2_OK) break;
+  }
+  if (ms_per_step) *ms_per_step = total_steps ? total_ms / total_steps : 0.0;
+  return rc;
+}
+
 // ---- reference-mirror API over one process-wide simulation ------------------------------
 static fg2_sim *g_sim = nullptr;
 static void g_done(void) { fg2_sim_destroy(g_sim); g_sim = nullptr; }

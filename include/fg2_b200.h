@@ -135,6 +135,11 @@ void *fg2_sim_stream(fg2_sim *s);
 /* dump()/load() (src/io.cpp:24-76): the reference's .raw frame format. */
 int fg2_sim_dump(fg2_sim *s, const char *path, double time);
 int fg2_sim_load(fg2_sim *s, const char *path, double *time);
+/* solve() (src/solve.cpp:25-64): frames i+1 .. n evenly spaced from t to t_final, each
+ * stepped to its time and dumped as <dir>/%04d.raw; the time step follows the getdt mode
+ * (FG2_DT_CFL: device-resident).  A NaN dumps <dir>/****.raw and returns FG2_ERR_NAN.
+ * ms_per_step (optional): the device time per step. */
+int fg2_sim_solve(fg2_sim *s, double t, double t_final, int i, int n, const char *dir, double *ms_per_step);
 
 /* ---- batches of independent simulations --------------------------------------------------
  * No single counterpart in the reference, which advances one grid per process

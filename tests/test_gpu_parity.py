@@ -128,6 +128,46 @@ def test_small_plain_configuration_100_steps(cuda):
     assert np.all(err_gpu <= np.maximum(3 * err_cpu, 1e-7)), (err_gpu, err_cpu)
 
 
+def test_solve_frames_match_manual_steps(tmp_path, cuda):
+    """solve() (src/solve.cpp:25-64) with the reference's getdt: the same steps as stepping by
+    hand, frames dumped as %04d.raw with their times, the last step of each frame shortened."""
+    n1, n2 = 48, 64
+    with fg2_b200.Sim(n1, n2) as a, fg2_b200.Sim(n1, n2) as b:
+        for s in (a, b):
+            s.config()
+            s.init("noise", seed=4)
+        dt = a.getdt()
+        t_final = 7.5 * dt
+        rc, ms = a.solve(0.0, t_final, 0, 3, tmp_path)
+        assert rc == 0 and ms > 0
+        t = 0.0
+        for k in range(1, 4):
+            target = t_final - (3 - k) * (t_final / 3)
+            while t < target:
+                h = min(target - t, dt)
+                assert b.step(t, h) == 0
+                t = min(t + h, target)
+            with fg2_b200.Sim(n1, n2) as c:
+                c.config()
+                assert c.load(tmp_path / f"{k:04d}.raw") == pytest.approx(target)
+                assert np.array_equal(c.download(), b.download())
+        assert np.array_equal(a.download(), b.download())
+
+
+def test_solve_with_device_cfl_steps(tmp_path, cuda):
+    with fg2_b200.Sim(64, 64) as s:
+        s.config()
+        s.init("kh", seed=2)
+        s.set_dt_mode("cfl")
+        rc, _ = s.solve(0.0, 2e-3, 0, 2, tmp_path)
+        assert rc == 0
+        assert s.time() == pytest.approx(2e-3, rel=1e-12)
+        for k in (1, 2):
+            with fg2_b200.Sim(64, 64) as c:
+                c.config()
+                assert c.load(tmp_path / f"{k:04d}.raw") == pytest.approx(1e-3 * k, rel=1e-12)
+
+
 def test_fused_step_equals_reference_building_blocks(cuda):
     """step() == Euler + 3 x (bcond, kick, drift) through the separate entry points."""
     n1, n2 = 48, 40
