@@ -67,6 +67,7 @@ def _bind(lib):
         "fg2_Euler": (None, [P, ctypes.c_float]), "fg2_global": (P, []),
         "fg2_sums_noalloc": (I, [P, I, I, LL, I, P, P]),
         "fg2_sim_solve": (I, [P, D, D, I, I, S, ctypes.POINTER(D)]),
+        "fg2_sim_test_stall_waits": (I, [P, I]),
         "fg2_batch_create": (P, [I, P, P, I, P]), "fg2_batch_destroy": (None, [P]),
         "fg2_batch_count": (I, [P]), "fg2_batch_cells": (LL, [P]), "fg2_batch_device_bytes": (SZ, [P]),
         "fg2_batch_stream": (P, [P]), "fg2_batch_member": (P, [P, I]),
@@ -248,6 +249,11 @@ class Sim:
 
     def clear_status(self):
         self.lib.fg2_sim_clear_status(self.h)
+
+    def test_stall_waits(self, nbytes):
+        """Tests of the timeout path: every data chunk of the substage kernel then waits for
+        `nbytes` more than its copies deliver, so its bounded waits run out (0 restores)."""
+        self._check(self.lib.fg2_sim_test_stall_waits(self.h, int(nbytes)), "test_stall_waits")
 
     def kick(self, t, beta):
         self._check(self.lib.fg2_sim_kick(self.h, float(t), float(beta)), "kick")

@@ -92,6 +92,7 @@ struct KParams {
   Status *status;        // launch errors
   int nb;                // output blocks of 7 rows per tile
   int reverse;           // tiles last first
+  unsigned wait_test_bytes;  // extra bytes every chunk expects (timeout-path tests; 0 otherwise)
   double comp_bg;        // beta * gamma of the next stage (16-bit residual carry), or 0
 };
 
@@ -149,6 +150,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
   kp.comp_bg = a.comp_bg;
   kp.reverse = a.reverse;
+  kp.wait_test_bytes = a.wait_test_bytes;
   return kp;
 }
 

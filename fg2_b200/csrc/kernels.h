@@ -30,6 +30,8 @@ struct StageArgs {
                         // residual into that stage through v (0: no next stage)
   int reverse = 0;      // take the tiles last first (alternated from launch to launch, so a
                         // stage starts on the tiles the previous one wrote last, still in L2)
+  unsigned wait_test_bytes = 0;  // tests of the timeout path: every chunk expects this many
+                                 // bytes more than arrive, so every bounded wait runs out
 };
 
 enum StageKind : int {

@@ -96,6 +96,7 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p2 = s->p2;
   a.status = s->status;
   a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
+  a.wait_test_bytes = s->wait_test_bytes;
   return a;
 }
 
@@ -733,6 +734,14 @@ double fg2_sim_last_dt(fg2_sim *s)
 {
   if (!s || read_status(s) < 0) return NAN;
   return s->status_host->dt_next;
+}
+
+int fg2_sim_test_stall_waits(fg2_sim *s, int bytes)
+{
+  if (!s || bytes < 0 || bytes > 4096) return fail(FG2_ERR_ARG, "bad arguments");
+  s->wait_test_bytes = (unsigned)bytes;
+  drop_graph(s);
+  return FG2_OK;
 }
 
 void fg2_sim_clear_status(fg2_sim *s)

@@ -33,6 +33,7 @@ struct fg2_sim {
   bool desc_valid = false;
   unsigned version = 0;       // bumped whenever settings that descriptors depend on change
   int order = 0;              // tile order of the next substage launch (alternates)
+  unsigned wait_test_bytes = 0;  // timeout-path tests (fg2_sim_test_stall_waits)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
   bool own_stream = false;

@@ -539,7 +539,7 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 template <class S, bool READ_V>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
-                                            bool reverse, int *queue)
+                                            bool reverse, unsigned extra_bytes, int *queue)
 {
   using G = Geo<S, READ_V>;
   if (ps->done) return;
@@ -566,7 +566,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     const GridDesc &gd = grids[ps->g];
     const int i0 = ps->i0, j0 = ps->j0, c = ps->c;
     const bool with_v = READ_V && c > 0;
-    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u));
+    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + extra_bytes);
     // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
     // columns j0 - 4 .. (padded column j0)
     tma_load_3d(smem + (size_t)s * G::SLOT, &gd.tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
@@ -688,7 +688,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1)
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, queue);
+    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);
   }
   __syncthreads();
 
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1)
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, queue);  // refill slot s
+      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }

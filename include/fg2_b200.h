@@ -112,6 +112,11 @@ int fg2_sim_set_time(fg2_sim *s, double t);   /* device clock for device-residen
 double fg2_sim_time(fg2_sim *s);              /* device clock (synchronises) */
 double fg2_sim_last_dt(fg2_sim *s);           /* last device-chosen dt (synchronises) */
 void fg2_sim_clear_status(fg2_sim *s);        /* clear the sticky NaN / error words */
+/* No counterpart in the reference.  For tests of the timeout path: with bytes > 0 every data
+ * chunk of the substage kernel waits for `bytes` more than its copies deliver, so each bounded
+ * in-kernel wait (2 s) runs out and the step returns FG2_ERR_TIMEOUT without faulting the GPU;
+ * 0 restores normal operation. */
+int fg2_sim_test_stall_waits(fg2_sim *s, int bytes);
 /* The reference's building blocks on the handle's current arrays. */
 int fg2_sim_kick(fg2_sim *s, double t, double beta); /* v <- F(u) + beta v  (src/kick.cu:108-114) */
 int fg2_sim_drift(fg2_sim *s, double dt);            /* u <- u + dt v        (src/drift.cu:34-39) */
