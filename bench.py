@@ -364,6 +364,45 @@ def run_mixed_leg(state, steps, warmup, device, plain_value):
     return out
 
 
+DISK_N = 2048
+DISK_DT = 1.0e-7  # inside the explicit radiation-diffusion limit (~0.28 Delta^2 = 6.6e-7 here)
+DISK_FLOP = 3 * (733 + 2 * 6)  # the reference's flop model per cell-step (src/config.cpp:33)
+DISK_B_ALG = 10 * 6 * 4  # 240 B per cell-step (six FP32 fields)
+
+
+def run_disk_leg(steps, warmup, device):
+    """The disk scheme (six fields, log-r / theta grid, 733-flop right-hand side) at
+    2048 x 2048 on the smooth torus-like state, FP32, fixed dt, steps replayed from the
+    two-step CUDA graph.  Compute-heavy: reported against the reference's flop model and
+    against HBM."""
+    import torch
+    import fg2_b200
+    peak, _ = peaks()
+    with fg2_b200.Sim(DISK_N, DISK_N, scheme="disk") as sim:
+        sim.config()
+        sim.init("smooth", seed=3)
+        stream = torch.cuda.ExternalStream(sim.stream, device=device)
+        sim.set_time(0.0)
+        sim.advance(max(warmup, 3), DISK_DT, graph=True)
+        if sim.sync() != 0:
+            raise RuntimeError("disk warm-up produced a bad status")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.advance(steps, DISK_DT, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        status = sim.sync()
+    cells = DISK_N * DISK_N
+    value = cells * steps / (ms / 1e3) / 1e9
+    return {"workload": f"disk {DISK_N}x{DISK_N} smooth torus-like state (seed 3), FP32, fixed dt {DISK_DT:g}, walls",
+            "value": value, "unit": "Gcell-steps/s", "steps": steps, "ms_per_step": ms / steps, "status": status,
+            "gflops_ref_model": value * DISK_FLOP, "flop_per_cell_step": DISK_FLOP,
+            "roofline": {"bound": "compute", "bytes_per_cell_step": DISK_B_ALG, "hbm_achieved": value * DISK_B_ALG,
+                         "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak}}
+
+
 def run_precision_leg(n, steps, device):
     """Kelvin-Helmholtz at n x n, the same fixed step sequence in FP64, FP32 and the 16-bit
     deviation storages; per-field L2 (RMS) and Linf errors against the FP64 run, and the
@@ -502,6 +541,10 @@ def run_fused(args):
         tiling = tuple(int(x) for x in args.batch_tiling.split(",")) if args.batch_tiling else None
         print(json.dumps(run_batch_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling, False)), flush=True)
         return
+    if args.only_disk:  # the disk-scheme leg alone (profiling)
+        torch.cuda.set_device(0)
+        print(json.dumps(run_disk_leg(args.steps, args.warmup, torch.device("cuda", 0))), flush=True)
+        return
 
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
@@ -573,6 +616,10 @@ def run_fused(args):
         precision = run_precision_leg(8192, 500, device)
         combined = run_combined_leg(device)
 
+    disk = None
+    if rank == 0 and world == 1 and not args.no_disk and args.storage == "f32":
+        disk = run_disk_leg(200, args.warmup, device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
@@ -603,6 +650,7 @@ def run_fused(args):
             "mixed": mixed,
             "precision": precision,
             "combined": combined,
+            "disk": disk,
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }
@@ -622,6 +670,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch (secondary) leg")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 16-bit storage and precision legs")
+    ap.add_argument("--no-disk", action="store_true", help="skip the disk-scheme leg")
+    ap.add_argument("--only-disk", action="store_true", help="run the disk-scheme leg alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="", help="nb,ctas_per_sm for the batch leg (default: autotune)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],

@@ -93,7 +93,7 @@ struct ParaKey {
 
 // Per-launch parameters of a scheme, by slot: the runtime keys first, then constants the
 // scheme derives from them on the host (scheme::derive), at most NPARA in all.
-constexpr int NPARA = 12;
+constexpr int NPARA = 24;
 template <class C>
 struct Para {
   C v[NPARA];
@@ -117,6 +117,7 @@ enum ErrorBits : unsigned { ERR_TMA_TIMEOUT = 1u, ERR_QUEUE_TIMEOUT = 2u };
 // images).  Fields whose sign flips at a reflecting wall have bg = 0, so a ghost image is the
 // negated 16-bit number.  v (the RK3 register) is stored as plain 16-bit numbers.
 constexpr int SCALE_TILE = 64;
+constexpr int DEV_MAX_FIELDS = 4;  // the codes hold one background and scale per field
 struct DevCode {
   float bg[4];           // per-field background (field mean at upload)
   const float4 *scale;   // per tile, row-major over (n1 / 64, n2 / 64) tiles: s of each field

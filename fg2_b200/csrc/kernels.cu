@@ -199,12 +199,17 @@ __device__ __noinline__ void store_ghosts(T *u, const Layout L, int i, int j, co
     }
 }
 
+// CFL signal rate of a cell (the scheme's: (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2 on a
+// Cartesian grid, from the cell's position on a curvilinear one).
 template <class C>
-__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2)
+__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2, int i, int j, C d1, C d2)
 {
-  const C cs = scheme::sound_speed(q, p);
-  return fmac(vabs(q[scheme::U1]) + cs, inv1, (vabs(q[scheme::U2]) + cs) * inv2);
+  return scheme::signal_rate<C>(q, p, inv1, inv2, i, j, d1, d2);
 }
+
+// 16-bit deviation storage codes hold at most DEV_MAX_FIELDS fields per cell; kernels for
+// 16-bit arrays are only compiled for schemes within that.
+constexpr bool DEV_OK = NV <= DEV_MAX_FIELDS;
 
 #include "substage.cuh"
 
@@ -279,6 +284,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   d->inv22 = 1.0 / (delta2 * delta2);
   d->inv12 = 1.0 / (delta1 * delta2);
   d->delta1 = delta1;
+  d->delta2 = delta2;
   if (dev) d->dev = *dev;
   else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0};
   return CUDA_SUCCESS;
@@ -356,8 +362,12 @@ cudaError_t launch_substage(int storage, int kind, bool cfl, bool scaled, const 
   switch (storage) {
     case ST_F32: return substage_s<float>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
     case ST_F64: return substage_s<double>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
-    case ST_F16: return substage_s<__half>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
-    case ST_BF16: return substage_s<__nv_bfloat16>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+    case ST_F16:
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else return substage_s<__half>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
+    case ST_BF16:
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else return substage_s<__nv_bfloat16>(kind, cfl, scaled, grids, ngrids, ntiles, a, queue, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -454,7 +464,7 @@ __device__ __forceinline__ double value_at(const S *u, const Layout &L, const De
 // getdt's reduction in FP64: max over cells of (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
 template <class T>
 __global__ void signal_max_kernel(const T *u, const Layout L, const Para<double> p, double inv1, double inv2,
-                                  Status *st, const DevCode dc)
+                                  double d1, double d2, Status *st, const DevCode dc)
 {
   const long long n = (long long)L.n1 * L.n2;
   double m = 0.0;
@@ -463,8 +473,12 @@ __global__ void signal_max_kernel(const T *u, const Layout L, const Para<double>
     double q[NV];
 #pragma unroll
     for (int f = 0; f < NV; ++f) q[f] = value_at<T>(u, L, dc, f, i, j);
-    const double cs = scheme::sound_speed<double>(q, p);
-    m = fmax(m, (fabs(q[scheme::U1]) + cs) * inv1 + (fabs(q[scheme::U2]) + cs) * inv2);
+    if constexpr (scheme::CURVILINEAR) {
+      m = fmax(m, scheme::signal_rate<double>(q, p, inv1, inv2, i, j, d1, d2));
+    } else {
+      const double cs = scheme::sound_speed<double>(q, p);
+      m = fmax(m, (fabs(q[scheme::U1]) + cs) * inv1 + (fabs(q[scheme::U2]) + cs) * inv2);
+    }
   }
 #pragma unroll
   for (int s = 16; s > 0; s >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, s));
@@ -655,13 +669,17 @@ cudaError_t launch_signal_max(int storage, const void *u, const Layout &L, const
   Para<double> p;
   for (int q = 0; q < NPARA; ++q) p.v[q] = para[q];
   const DevCode dc = dev ? *dev : DevCode{};
-  const double i1 = 1.0 / delta1, i2 = 1.0 / delta2;
+  const double i1 = 1.0 / delta1, i2 = 1.0 / delta2, d1 = delta1, d2 = delta2;
   switch (storage) {
-    case ST_F32: signal_max_kernel<float><<<g, 256, 0, s>>>((const float *)u, L, p, i1, i2, st, dc); break;
-    case ST_F64: signal_max_kernel<double><<<g, 256, 0, s>>>((const double *)u, L, p, i1, i2, st, dc); break;
-    case ST_F16: signal_max_kernel<__half><<<g, 256, 0, s>>>((const __half *)u, L, p, i1, i2, st, dc); break;
+    case ST_F32: signal_max_kernel<float><<<g, 256, 0, s>>>((const float *)u, L, p, i1, i2, d1, d2, st, dc); break;
+    case ST_F64: signal_max_kernel<double><<<g, 256, 0, s>>>((const double *)u, L, p, i1, i2, d1, d2, st, dc); break;
+    case ST_F16:
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else signal_max_kernel<__half><<<g, 256, 0, s>>>((const __half *)u, L, p, i1, i2, d1, d2, st, dc);
+      break;
     case ST_BF16:
-      signal_max_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16 *)u, L, p, i1, i2, st, dc);
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else signal_max_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((const __nv_bfloat16 *)u, L, p, i1, i2, d1, d2, st, dc);
       break;
     default: return cudaErrorInvalidValue;
   }
@@ -676,9 +694,13 @@ cudaError_t launch_sums(int storage, const void *u, const Layout &L, double *par
   switch (storage) {
     case ST_F32: sums_kernel<float><<<nb, SUM_THREADS, 0, s>>>((const float *)u, L, partials, dc); break;
     case ST_F64: sums_kernel<double><<<nb, SUM_THREADS, 0, s>>>((const double *)u, L, partials, dc); break;
-    case ST_F16: sums_kernel<__half><<<nb, SUM_THREADS, 0, s>>>((const __half *)u, L, partials, dc); break;
+    case ST_F16:
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else sums_kernel<__half><<<nb, SUM_THREADS, 0, s>>>((const __half *)u, L, partials, dc);
+      break;
     case ST_BF16:
-      sums_kernel<__nv_bfloat16><<<nb, SUM_THREADS, 0, s>>>((const __nv_bfloat16 *)u, L, partials, dc);
+      if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+      else sums_kernel<__nv_bfloat16><<<nb, SUM_THREADS, 0, s>>>((const __nv_bfloat16 *)u, L, partials, dc);
       break;
     default: return cudaErrorInvalidValue;
   }
@@ -690,22 +712,28 @@ cudaError_t launch_encode(int storage, void *u, const float *src, const Layout &
 {
   const int g = grid_for((long long)L.n1 * L.n2 * NV, 256);
   const DevCode dc = dev ? *dev : DevCode{};
-  if (storage == ST_F16) encode_kernel<__half><<<g, 256, 0, s>>>((__half *)u, src, L, dc, dev != nullptr);
-  else if (storage == ST_BF16)
-    encode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((__nv_bfloat16 *)u, src, L, dc, dev != nullptr);
-  else return cudaErrorInvalidValue;
-  return cudaGetLastError();
+  if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+  else {
+    if (storage == ST_F16) encode_kernel<__half><<<g, 256, 0, s>>>((__half *)u, src, L, dc, dev != nullptr);
+    else if (storage == ST_BF16)
+      encode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>((__nv_bfloat16 *)u, src, L, dc, dev != nullptr);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
 }
 
 cudaError_t launch_decode(int storage, float *dst, const void *u, const Layout &L, const DevCode *dev, cudaStream_t s)
 {
   const int g = grid_for((long long)L.n1 * L.n2 * NV, 256);
   const DevCode dc = dev ? *dev : DevCode{};
-  if (storage == ST_F16) decode_kernel<__half><<<g, 256, 0, s>>>(dst, (const __half *)u, L, dc, dev != nullptr);
-  else if (storage == ST_BF16)
-    decode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>(dst, (const __nv_bfloat16 *)u, L, dc, dev != nullptr);
-  else return cudaErrorInvalidValue;
-  return cudaGetLastError();
+  if constexpr (!DEV_OK) return cudaErrorInvalidValue;
+  else {
+    if (storage == ST_F16) decode_kernel<__half><<<g, 256, 0, s>>>(dst, (const __half *)u, L, dc, dev != nullptr);
+    else if (storage == ST_BF16)
+      decode_kernel<__nv_bfloat16><<<g, 256, 0, s>>>(dst, (const __nv_bfloat16 *)u, L, dc, dev != nullptr);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
 }
 
 cudaError_t launch_dt_update_batch(Status *st, const double2 *limits, int count, double t_end, cudaStream_t s)

@@ -57,7 +57,7 @@ struct GridDesc {
   Status *status;         // NaN flag and CFL max of this grid
   double inv1, inv2;      // 1 / Delta per axis (batch launches scale by these)
   double inv11, inv22, inv12;  // 1 / (Delta1 Delta1), 1 / (Delta2 Delta2), 1 / (Delta1 Delta2)
-  double delta1;          // Delta1
+  double delta1, delta2;  // Delta1, Delta2 (curvilinear schemes place cells by them)
   DevCode dev;            // deviation-storage codes (FP16 / BF16 arrays)
 };
 

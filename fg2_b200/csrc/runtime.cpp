@@ -131,7 +131,13 @@ int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridD
 int ensure_config(fg2_sim *s)
 {
   if (!s->configured) {
-    scheme::settings(s->l1, s->l2);
+    const int p1 = s->p1, p2 = s->p2;
+    if (s->storage == ST_F64) scheme::settings<double>(s->n1, s->n2, s->l1, s->l2, s->p1, s->p2);
+    else scheme::settings<float>(s->n1, s->n2, s->l1, s->l2, s->p1, s->p2);
+    if (s->p1 != p1 || s->p2 != p2) {  // a scheme that fixes its boundaries (src/config.cpp:26)
+      s->ghosts_valid = false;
+      drop_graph(s);
+    }
     compute_deltas(s);
     s->configured = true;
   }
@@ -316,7 +322,8 @@ int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, c
   for (int q = 0; q < scheme::NSLOT; ++q)
     p[scheme::PARA_KEYS[q].slot] = para ? para[q] : scheme::PARA_KEYS[q].def;
   scheme::derive(p);
-  scheme::settings(l1, l2);
+  int p1 = BC_PERIODIC, p2 = BC_PERIODIC;
+  scheme::settings<double>(n1, n2, l1, l2, p1, p2);
   SetupCtx ctx{n1, n2, l1, l2, p, seed};
   std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
   const size_t row = (size_t)n2 * scheme::NVAR;
@@ -343,6 +350,11 @@ fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_a
   }
   if (storage != ST_F32 && storage != ST_F64 && storage != ST_F16 && storage != ST_BF16) {
     fail(FG2_ERR_UNSUPPORTED, "unknown storage %d", storage);
+    return nullptr;
+  }
+  if ((storage == ST_F16 || storage == ST_BF16) && scheme::NVAR > DEV_MAX_FIELDS) {
+    fail(FG2_ERR_UNSUPPORTED, "16-bit deviation storage holds at most 4 fields per cell; scheme %s has %d",
+         scheme::NAME, scheme::NVAR);
     return nullptr;
   }
   std::unique_ptr<fg2_sim> s(new fg2_sim);

@@ -36,11 +36,11 @@ inline unsigned d2_fields(const double *v)
 
 // dq/dt at one cell (or cell pair in the same row i; Kolmogorov forcing varies with i).
 template <unsigned M2, class C>
-FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1)
+FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2)
 {
   using fg2::fmac;
   using fg2::lit;
-  (void)j;
+  (void)j; (void)delta2;
   const C u1 = c.q[U1], u2 = c.q[U2];
   const C div = c.d1[U1] + c.d2[U2];
   const C m1 = lit<C>(-1.0);
@@ -74,6 +74,15 @@ FG2_HD C sound_speed(const C q[NVAR], const fg2::Para<C> &p)
 {
   (void)q;
   return p.v[CS];
+}
+
+// CFL signal rate of a cell on the Cartesian grid: (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
+template <class C>
+FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2)
+{
+  (void)i; (void)j; (void)delta1; (void)delta2;
+  const C cs = sound_speed<C>(q, p);
+  return fg2::fmac(fg2::vabs(q[U1]) + cs, inv1, (fg2::vabs(q[U2]) + cs) * inv2);
 }
 
 inline double max_diffusivity(const double *v)

@@ -7,6 +7,8 @@ namespace scheme {
 constexpr const char *NAME = "hydro-isot";
 constexpr int NVAR = 3;
 enum Field { LND = 0, U1 = 1, U2 = 2 };
+// Cartesian grid: the CFL rate needs no cell position.
+constexpr bool CURVILINEAR = false;
 constexpr const char *FIELD_NAMES[NVAR] = {"lnd", "u1", "u2"};
 
 }  // namespace scheme

@@ -43,13 +43,13 @@ inline unsigned d2_fields(const double *v)
 }
 
 // dq/dt at one cell (or cell pair).  M2 is the set of fields whose D11/D22 the caller
-// evaluated; the others read as zero.  i, j, delta1 are unused by this scheme.
+// evaluated; the others read as zero.  i, j and the spacings are unused by this scheme.
 template <unsigned M2, class C>
-FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1)
+FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2)
 {
   using fg2::fmac;
   using fg2::lit;
-  (void)i; (void)j; (void)delta1;
+  (void)i; (void)j; (void)delta1; (void)delta2;
   const C u1 = c.q[U1], u2 = c.q[U2];
   const C ee = fg2::vexp(c.q[LNE]);    // specific thermal energy e
   const C iee = fg2::vexp(-c.q[LNE]);  // (gamma - 1) / temp = 1 / e
@@ -91,6 +91,15 @@ template <class C>
 FG2_HD C sound_speed(const C q[NVAR], const fg2::Para<C> &p)
 {
   return p.v[CSG] * fg2::vexp(q[LNE] * fg2::lit<C>(0.5));
+}
+
+// CFL signal rate of a cell on the Cartesian grid: (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
+template <class C>
+FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2)
+{
+  (void)i; (void)j; (void)delta1; (void)delta2;
+  const C cs = sound_speed<C>(q, p);
+  return fg2::fmac(fg2::vabs(q[U1]) + cs, inv1, (fg2::vabs(q[U2]) + cs) * inv2);
 }
 
 // Largest diffusion coefficient in the equations, for the explicit diffusive limit:

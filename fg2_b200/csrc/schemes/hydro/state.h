@@ -7,6 +7,8 @@ namespace scheme {
 constexpr const char *NAME = "hydro";
 constexpr int NVAR = 4;
 enum Field { LND = 0, U1 = 1, U2 = 2, LNE = 3 };
+// Cartesian grid: the CFL rate needs no cell position.
+constexpr bool CURVILINEAR = false;
 constexpr const char *FIELD_NAMES[NVAR] = {"lnd", "u1", "u2", "lne"};
 
 }  // namespace scheme

@@ -67,7 +67,16 @@ constexpr int NCW = SW / 32;       // warps per CTA
 constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
 constexpr int NP = (NV + 1) / 2;   // field pairs
 static_assert(NT == SW, "one thread per strip column");
-static_assert(scheme::U1 == 1 && scheme::U2 == 2, "u1 and u2 are fields 1 and 2");
+
+// Fields with a mixed derivative D12 (the scheme's D12_FIELDS), in field order: the k-th of
+// them has streaming accumulator k.
+__host__ __device__ constexpr int d12_count(unsigned m) { return m ? (int)(m & 1u) + d12_count(m >> 1) : 0; }
+__host__ __device__ constexpr int d12_field(unsigned m, int k, int f = 0)
+{
+  return (m & 1u) ? (k == 0 ? f : d12_field(m >> 1, k - 1, f + 1)) : d12_field(m >> 1, k, f + 1);
+}
+constexpr int ND12 = d12_count(scheme::D12_FIELDS);
+static_assert(ND12 >= 1 && d12_field(scheme::D12_FIELDS, ND12 - 1) < NV, "mixed-derivative fields");
 
 // Cells per TMA group of a storage type: the innermost box dimension is one group of
 // interleaved cells and must be a multiple of 16 bytes.
@@ -115,6 +124,9 @@ __device__ __forceinline__ void ld_cell(const T *p, typename PairOf<T>::type out
   } else if constexpr (NV == 4 && sizeof(T) == 8) {
     out[0] = *reinterpret_cast<const double2 *>(p);
     out[1] = *reinterpret_cast<const double2 *>(p + 2);
+  } else if constexpr (NV == 6) {  // 24- or 48-byte cells: three 8- or 16-byte accesses
+#pragma unroll
+    for (int q = 0; q < 3; ++q) out[q] = *reinterpret_cast<const typename PO::type *>(p + 2 * q);
   } else {
 #pragma unroll
     for (int q = 0; q < NP; ++q) out[q] = PO::make(p[2 * q], 2 * q + 1 < NV ? p[2 * q + 1] : T(0));
@@ -129,6 +141,9 @@ __device__ __forceinline__ void st_cell(T *p, const typename PairOf<T>::type in[
   } else if constexpr (NV == 4 && sizeof(T) == 8) {
     *reinterpret_cast<double2 *>(p) = in[0];
     *reinterpret_cast<double2 *>(p + 2) = in[1];
+  } else if constexpr (NV == 6) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) *reinterpret_cast<typename PairOf<T>::type *>(p + 2 * q) = in[q];
   } else {
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
@@ -244,7 +259,7 @@ struct Roll {
   P w[NP][CH];    // u(row, j) per field pair, rows L-6 .. L
   P h2[NP][CH];   // D2 of each row
   P h22[NP][CH];  // D22 of each row (only the lanes under the mask are written)
-  T x[2][CH];     // D12 accumulators of u1, u2
+  T x[ND12][CH];  // D12 accumulators of the D12 fields
 };
 
 // Everything a thread needs of the grid its current tile belongs to (registers).
@@ -258,7 +273,7 @@ struct GridRegs {
   int p1, p2;
   P gdt;                       // gamma dt of this grid's step, both lanes
   P s1, s2, s11, s22;          // 1/Delta factors (batch launches)
-  T s12, inv1, inv2, delta1;   // 1/(Delta1 Delta2), CFL factors, Delta1
+  T s12, inv1, inv2, delta1, delta2;  // 1/(Delta1 Delta2), CFL factors, Delta1, Delta2
   // deviation storage
   P bg[NP];                    // per-field background
   P comp;                      // 1 / (beta' gamma' dt) of the next stage, or 0
@@ -296,6 +311,39 @@ __device__ __forceinline__ void lead_pair(const typename PairOf<T>::type (&x)[7]
   }
 }
 
+// D12 of D12 field number G (field f is lane f & 1 of pair f / 2) from the leading row's
+// differences: rows L+k get -m_k delta_k(L) (mn = -m), rows L-k get +m_k delta_k(L); row L-3
+// is then complete.  The first contribution to row L+3 initialises its accumulator.  One
+// instantiation per field, so every index is a compile-time constant.
+template <class T, int R, int G>
+__device__ __forceinline__ void d12_lead(const typename PairOf<T>::type (&dk)[NP][3], const KParams<T> &a, Roll<T> &s)
+{
+  if constexpr (G < ND12) {
+    constexpr int f = d12_field(scheme::D12_FIELDS, G), pf = f >> 1;
+    const T d1 = (f & 1) ? dk[pf][0].y : dk[pf][0].x;
+    const T d2 = (f & 1) ? dk[pf][1].y : dk[pf][1].x;
+    const T d3 = (f & 1) ? dk[pf][2].y : dk[pf][2].x;
+    s.x[G][(R + 3) % CH] = a.ks.mn[2] * d3;
+    s.x[G][(R + 2) % CH] = fmac(a.ks.mn[1], d2, s.x[G][(R + 2) % CH]);
+    s.x[G][(R + 1) % CH] = fmac(a.ks.mn[0], d1, s.x[G][(R + 1) % CH]);
+    s.x[G][(R + 6) % CH] = fmac(a.ks.m[0], d1, s.x[G][(R + 6) % CH]);
+    s.x[G][(R + 5) % CH] = fmac(a.ks.m[1], d2, s.x[G][(R + 5) % CH]);
+    s.x[G][(R + 4) % CH] = fmac(a.ks.m[2], d3, s.x[G][(R + 4) % CH]);
+    d12_lead<T, R, G + 1>(dk, a, s);
+  }
+}
+
+// The finished D12 of every D12 field at output slot S0 into the cell (other fields: 0).
+template <class T, bool SC, int S0, int G, class GR>
+__device__ __forceinline__ void d12_emit(const GR &gr, const Roll<T> &s, Cell<T, NV> &cell)
+{
+  if constexpr (G < ND12) {
+    constexpr int f = d12_field(scheme::D12_FIELDS, G);
+    cell.d12[f] = SC ? s.x[G][S0] * gr.s12 : s.x[G][S0];
+    d12_emit<T, SC, S0, G + 1>(gr, s, cell);
+  }
+}
+
 // Leading-row work for register slot R: loads the 7 cells of row R of the chunk around the
 // thread's column; base points at column j-3 of row 0, rows are RSTRIDE elements apart.
 template <class T, unsigned M2, int R, int RSTRIDE>
@@ -309,21 +357,8 @@ __device__ __forceinline__ void lead_row(const T *base, const KParams<T> &a, Rol
   P dk[NP][3];
   lead_pair<T, M2, R, 0>(x, a, s, dk[0]);
   if constexpr (NP > 1) lead_pair<T, M2, R, 1>(x, a, s, dk[1]);
-  // D12 of u1 (pair 0, lane y) and u2 (pair 1, lane x): rows L+k get -m_k delta_k(L) (mn = -m),
-  // rows L-k get +m_k delta_k(L); row L-3 is then complete.  The first contribution to row
-  // L+3 initialises its accumulator.
-#pragma unroll
-  for (int g = 0; g < 2; ++g) {
-    const T d1 = g == 0 ? dk[0][0].y : dk[1][0].x;
-    const T d2 = g == 0 ? dk[0][1].y : dk[1][1].x;
-    const T d3 = g == 0 ? dk[0][2].y : dk[1][2].x;
-    s.x[g][(R + 3) % CH] = a.ks.mn[2] * d3;
-    s.x[g][(R + 2) % CH] = fmac(a.ks.mn[1], d2, s.x[g][(R + 2) % CH]);
-    s.x[g][(R + 1) % CH] = fmac(a.ks.mn[0], d1, s.x[g][(R + 1) % CH]);
-    s.x[g][(R + 6) % CH] = fmac(a.ks.m[0], d1, s.x[g][(R + 6) % CH]);
-    s.x[g][(R + 5) % CH] = fmac(a.ks.m[1], d2, s.x[g][(R + 5) % CH]);
-    s.x[g][(R + 4) % CH] = fmac(a.ks.m[2], d3, s.x[g][(R + 4) % CH]);
-  }
+  if constexpr (NP > 2) lead_pair<T, M2, R, 2>(x, a, s, dk[2]);
+  d12_lead<T, R, 0>(dk, a, s);
 }
 
 // Derivatives of field pair PI at the output row held in register slot S0, into a Cell.
@@ -377,12 +412,11 @@ __device__ __forceinline__ void emit_pair(const KParams<T> &a, const GR &gr, con
 // narrower than two ghost widths take the general path.  Out of line: only cells of tiles
 // near an edge call it, and one copy keeps the unrolled row loop small.
 template <class S>
-__device__ __noinline__ void rim_images(S *u, const Layout L, int i, int j, typename PairOf<typename Store<S>::C>::type q0,
-                                        typename PairOf<typename Store<S>::C>::type q1, int p1, int p2)
+__device__ __forceinline__ void rim_body(S *u, const Layout L, int i, int j,
+                                         const typename PairOf<typename Store<S>::C>::type (&qp)[NP], int p1, int p2)
 {
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
-  const P qp[2] = {q0, q1};
   const int n1 = L.n1, n2 = L.n2;
   if (n1 < 2 * HALF || n2 < 2 * HALF) {
     T qn[NV];
@@ -410,6 +444,27 @@ __device__ __noinline__ void rim_images(S *u, const Layout L, int i, int j, type
     store_cell<S>(u + L.at(0, i, ja), f);
     if (ia > -(1 << 30)) store_cell<S>(u + L.at(0, ia, ja), f);
   }
+}
+
+// Cells of up to two field pairs (q1 is the last pair) ...
+template <class S>
+__device__ __noinline__ void rim_images(S *u, const Layout L, int i, int j, typename PairOf<typename Store<S>::C>::type q0,
+                                        typename PairOf<typename Store<S>::C>::type q1, int p1, int p2)
+{
+  using P = typename PairOf<typename Store<S>::C>::type;
+  const P qp[2] = {q0, q1};
+  if constexpr (NP <= 2) rim_body<S>(u, L, i, j, qp, p1, p2);
+}
+
+// ... and of three (six-field schemes).
+template <class S>
+__device__ __noinline__ void rim_images3(S *u, const Layout L, int i, int j, typename PairOf<typename Store<S>::C>::type q0,
+                                         typename PairOf<typename Store<S>::C>::type q1,
+                                         typename PairOf<typename Store<S>::C>::type q2, int p1, int p2)
+{
+  using P = typename PairOf<typename Store<S>::C>::type;
+  const P qp[3] = {q0, q1, q2};
+  if constexpr (NP == 3) rim_body<S>(u, L, i, j, qp, p1, p2);
 }
 
 // The same for 16-bit storage, with the stored numbers (reflected fields have bg = 0, so their
@@ -454,13 +509,14 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   Cell<T, NV> cell;
   emit_pair<T, M2, SC, S0, 0>(a, gr, s, cell);
   if constexpr (NP > 1) emit_pair<T, M2, SC, S0, 1>(a, gr, s, cell);
+  if constexpr (NP > 2) emit_pair<T, M2, SC, S0, 2>(a, gr, s, cell);
 #pragma unroll
   for (int f = 0; f < NV; ++f) cell.d12[f] = T(0);
-  cell.d12[scheme::U1] = SC ? s.x[0][S0] * gr.s12 : s.x[0][S0];
-  cell.d12[scheme::U2] = SC ? s.x[1][S0] * gr.s12 : s.x[1][S0];
+  d12_emit<T, SC, S0, 0>(gr, s, cell);
 
   T r[NV];
-  scheme::eqns<M2>(cell, a.p, i, j, r, SC ? gr.delta1 : a.ks.delta1);
+  const T dl1 = SC ? gr.delta1 : a.ks.delta1, dl2 = SC ? gr.delta2 : a.ks.delta2;
+  scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2);
   if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
   P vn[NP], qp[NP];
 #pragma unroll
@@ -506,10 +562,13 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
     for (int f = 1; f < NV; ++f) sum += qn[f];
     nan |= sum != sum;
     if (rim) {  // tiles within HALF cells of an edge: the cell's ghost images for the next stage
-      if constexpr (!St::DEV) rim_images<S>(gr.u_out, gr.L, i, j, qp[0], qp[NP - 1], gr.p1, gr.p2);
+      if constexpr (!St::DEV) {
+        if constexpr (NP == 3) rim_images3<S>(gr.u_out, gr.L, i, j, qp[0], qp[1], qp[2], gr.p1, gr.p2);
+        else rim_images<S>(gr.u_out, gr.L, i, j, qp[0], qp[NP - 1], gr.p1, gr.p2);
+      }
       else rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
     }
-    if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2));
+    if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2, i, j, dl1, dl2));
   }
 }
 
@@ -604,6 +663,7 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
     gr.inv1 = (T)gd.inv1;
     gr.inv2 = (T)gd.inv2;
     gr.delta1 = (T)gd.delta1;
+    gr.delta2 = (T)gd.delta2;
   } else {
     gr.inv1 = a.ks.inv1;
     gr.inv2 = a.ks.inv2;
@@ -666,7 +726,7 @@ __device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
 }
 
 template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
+__global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? (NV > 4 ? 2 : 3) : 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
                                                          const KParams<typename Store<S>::C> a, int *queue)
 {
   using T = typename Store<S>::C;
@@ -742,7 +802,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? 3 : 1)
     }
     if (b < 0) {
 #pragma unroll
-      for (int g2 = 0; g2 < 2; ++g2)
+      for (int g2 = 0; g2 < ND12; ++g2)
 #pragma unroll
         for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
       // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators

@@ -17,7 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HALO = 3
-SCHEMES = {"hydro": ("hydro", 4), "hydro-isot": ("isot", 3), "isot": ("isot", 3)}
+SCHEMES = {"hydro": ("hydro", 4), "hydro-isot": ("isot", 3), "isot": ("isot", 3), "disk": ("disk", 6)}
 
 
 def lib_path(scheme="hydro", prec="f32", kind="port"):
@@ -143,9 +143,27 @@ class Oracle:
 
 
 # Reference-default parameters and the box each scheme forces (src/hydro/eqns.cuh:19-24,
-# src/hydro-isot/eqns.cuh:19-25, src/hydro-isot/config.h:21-26, src/global.cpp:28).
-def default_box(scheme):
-    return (2 * np.pi, 2 * np.pi) if SCHEMES[scheme][0] == "isot" else (1.0, 1.0)
+# src/hydro-isot/eqns.cuh:19-25, src/hydro-isot/config.h:21-26, src/disk/config.h:24-34,
+# src/global.cpp:28).
+def default_box(scheme, n1=None, n2=None):
+    tag = SCHEMES[scheme][0]
+    if tag == "isot":
+        return (2 * np.pi, 2 * np.pi)
+    if tag == "disk":
+        return disk_box(n1, n2)
+    return (1.0, 1.0)
+
+
+def disk_box(n1, n2, f64=False):
+    """The disk scheme's box (src/disk/config.h:24-34): theta over the full pi wedge and a
+    log-r extent 2 n1 asinh(pi / (2 n2)) that makes the cells about square, evaluated with
+    R-typed intermediates (R = float unless f64)."""
+    R = np.float64 if f64 else np.float32
+    l2 = R(np.pi)
+    hd2 = R(0.5 * np.float64(l2) / n2)
+    hd1 = R(np.log(np.float64(hd2) + np.sqrt(np.float64(R(hd2 * hd2)) + 1.0)))
+    l1 = R(2.0 * np.float64(hd1) * n1)
+    return float(l1), float(l2)
 
 
 def reference_dt(n1, n2, l1, l2, c=0.5):

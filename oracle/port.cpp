@@ -3,10 +3,11 @@
  * the CUDA path; nothing in the product links it or calls it.
  *
  * A CPU restatement of fg2's 2D hydro time step: the 6th-order stencils of
- * src/deriv.h:39-63, the right-hand sides of src/hydro/eqns.cuh:26-92 and
- * src/hydro-isot/eqns.cuh:27-87, the Euler hooks of src/hydro/Euler.cuh:19-22 and
- * src/hydro-isot/Euler.cuh:24-37, the reflective sign maps of src/hydro/bcond.cuh:19-28 and src/hydro-isot/bcond.cuh:19-28,
- * and (through oracle/loops.h) the kick / drift / bcond / step loops.
+ * src/deriv.h:39-63, the right-hand sides of src/hydro/eqns.cuh:26-92,
+ * src/hydro-isot/eqns.cuh:27-87 and src/disk/eqns.cuh:38-247, the Euler hooks of
+ * src/hydro/Euler.cuh:19-22, src/hydro-isot/Euler.cuh:24-37 and src/disk/Euler.cuh:19-69,
+ * the reflective sign maps of src/hydro/bcond.cuh:19-28, src/hydro-isot/bcond.cuh:19-28 and
+ * src/disk/bcond.cuh:19-29, and (through oracle/loops.h) the kick / drift / bcond / step loops.
  *
  * Every expression keeps the reference's evaluation order, so that with
  * -ffp-contract=off this file and oracle/ref_harness.cpp (the reference's own headers
@@ -14,7 +15,8 @@
  * against the committed golden vectors.
  *
  * Build variants (oracle/Makefile): ORC_SCHEME=1 hydro (NVAR 4), ORC_SCHEME=2 hydro-isot
- * (NVAR 3); ORC_DOUBLE selects R=double / E=long double as -DDOUBLE does in src/fg2.h:36-45.
+ * (NVAR 3), ORC_SCHEME=3 disk (NVAR 6); ORC_DOUBLE selects R=double / E=long double as
+ * -DDOUBLE does in src/fg2.h:36-45.
  */
 #include <cmath>
 #include <cstdint>
@@ -39,8 +41,11 @@ struct S { R lnd, u1, u2, lne; };
 #elif ORC_SCHEME == 2
 #define NV 3
 struct S { R lnd, u1, u2; };
+#elif ORC_SCHEME == 3
+#define NV 6
+struct S { R lnd, ur, uz, Omg, lne, lner; };
 #else
-#error "ORC_SCHEME must be 1 (hydro) or 2 (hydro-isot)"
+#error "ORC_SCHEME must be 1 (hydro), 2 (hydro-isot) or 3 (disk)"
 #endif
 
 namespace {
@@ -146,7 +151,7 @@ void first_order(S *, R, int, int) {}
 // src/hydro/bcond.cuh:19-28: u2 flips sign at a reflective wall.
 R transform(int var, R x) { return var == U2 ? -x : x; }
 
-#else
+#elif ORC_SCHEME == 2
 // ---- hydro-isot: src/hydro-isot/eqns.cuh:19-25 (keys) and :27-87 (RHS) ---------------
 R p_dd = 0.0, p_nus = 2.0e-4, p_nub = 0.0, p_cs2 = 1.0, p_f = 0.0, p_k = -8.0;
 struct Key { const char *name; R *val; } keys[] = {{"dd", &p_dd},   {"nus", &p_nus}, {"nub", &p_nub},
@@ -204,6 +209,163 @@ void first_order(S *u, R dt, int i, int j)
 }
 
 R transform(int var, R x) { return var == U2 ? -x : x; }
+
+#else
+// ---- disk: src/disk/eqns.cuh:19-36 (keys) and :38-247 (RHS) --------------------------
+// Log-r / theta grid: axis 1 is ln(r / r_in), axis 2 is theta.  The expressions keep the
+// reference's order; sincos, exp, pow, sqrt and log are the precision-R library functions.
+R p_M = 1.0, p_rS = 2.0, p_rin = 3.0, p_gamma = 5.0 / 3.0, p_nus = 0.0, p_nub = 0.0, p_kappa = 0.0,
+  p_alpha = 0.01, p_ar = 1.0e+8, p_es = 1.0, p_ff = 0.0, p_dd = 1.0e-4, p_nu = 2.0e-4, p_ed = 5.0e-4,
+  p_rd = 5.0e-4;
+struct Key { const char *name; R *val; } keys[] = {
+    {"M", &p_M},     {"rS", &p_rS}, {"rin", &p_rin}, {"gamma", &p_gamma}, {"nus", &p_nus},
+    {"nub", &p_nub}, {"kappa", &p_kappa}, {"alpha", &p_alpha}, {"ar", &p_ar}, {"es", &p_es},
+    {"ff", &p_ff},   {"dd", &p_dd}, {"nu", &p_nu}, {"ed", &p_ed}, {"rd", &p_rd}};
+enum { UR = 1, UZ = 2, OMG = 3, LNE6 = 4, LNER = 5 };
+
+inline void sin_cos(float x, float *s, float *c) { sincosf(x, s, c); }
+inline void sin_cos(double x, double *s, double *c) { sincos(x, s, c); }
+
+S rhs(const S *c, int i, int j, int s)
+{
+  R sint, cost;
+  sin_cos((j + K(0.5)) * Delta2, &sint, &cost);
+  const R sphr = p_rin * std::exp((i + K(0.5)) * Delta1);
+  const R r = sphr * sint;  // cylindrical radius
+  const R sphr_2 = sphr * sphr;
+
+  const R den = std::exp(c->lnd), eng = std::exp(c->lne), rad = std::exp(c->lner);
+  const R gamma1 = p_gamma - K(1.0);
+  const R temp = gamma1 * eng;
+  const R nuSS = p_alpha * p_gamma * temp * r * std::sqrt(r / p_M);
+
+  // gradient in (R, z) from the (ln r, theta) derivatives
+  R dr[NV], dz[NV], d11v[NV], d22v[NV], lap[NV];
+  for (int f = 0; f < NV; ++f) {
+    const R g1 = d1(c, s, f), g2 = d2(c, s, f);
+    dr[f] = (sint * g1 + cost * g2) / sphr;
+    dz[f] = (cost * g1 - sint * g2) / sphr;
+  }
+  for (int f = 0; f < NV; ++f) { d11v[f] = d11(c, s, f); d22v[f] = d22(c, s, f); }
+  const R x_lnd = d12(c, s, LND), x_ur = d12(c, s, UR), x_uz = d12(c, s, UZ), x_lner = d12(c, s, LNER);
+  const R cr = cost / sphr, sr = sint / sphr;
+  const R cc = cr * cr, cs = cr * sr, ss = sr * sr;
+  const R c2 = cc - ss, s2 = K(2.0) * cs;
+  for (int f = 0; f < NV; ++f) lap[f] = (d11v[f] + d22v[f]) / sphr_2;
+  auto rr = [&](int f, R x) { return ss * d11v[f] + cc * d22v[f] + s2 * x + cr * dz[f] - sr * dr[f]; };
+  auto rz = [&](int f, R x) { return cs * (d11v[f] - d22v[f]) + c2 * x - cr * dr[f] - sr * dz[f]; };
+  auto zz = [&](int f, R x) { return cc * d11v[f] + ss * d22v[f] - s2 * x - cr * dz[f] + sr * dr[f]; };
+  const R drr_lnd = rr(LND, x_lnd), drr_ur = rr(UR, x_ur), drr_lner = rr(LNER, x_lner);
+  const R drz_lnd = rz(LND, x_lnd), drz_ur = rz(UR, x_ur), drz_uz = rz(UZ, x_uz), drz_lner = rz(LNER, x_lner);
+  const R dzz_lnd = zz(LND, x_lnd), dzz_uz = zz(UZ, x_uz), dzz_lner = zz(LNER, x_lner);
+
+  R t[NV] = {0, 0, 0, 0, 0, 0};
+  const R ur = c->ur, uz = c->uz, Omg = c->Omg;
+  // advection and pseudo-forces
+  t[LND] -= ur * dr[LND] + uz * dz[LND];
+  t[UR] -= ur * dr[UR] + uz * dz[UR] - Omg * Omg * r;
+  t[UZ] -= ur * dr[UZ] + uz * dz[UZ];
+  t[OMG] -= ur * dr[OMG] + uz * dz[OMG] + K(2.0) * ur * Omg / r;
+  t[LNE6] -= ur * dr[LNE6] + uz * dz[LNE6];
+  t[LNER] -= ur * dr[LNER] + uz * dz[LNER];
+  // compression and pressure
+  const R ur_r = c->ur / r;
+  const R div_u = dr[UR] + dz[UZ] + ur_r;
+  t[LND] -= div_u;
+  t[UR] -= temp * (dr[LND] + dr[LNE6]);
+  t[UZ] -= temp * (dz[LND] + dz[LNE6]);
+  t[LNE6] -= div_u * gamma1;
+  // density- and temperature-dependent viscous terms, viscous heating
+  const R Srr = dr[UR] - div_u / K(3.0);
+  const R Szz = dz[UZ] - div_u / K(3.0);
+  const R Spp = ur_r - div_u / K(3.0);
+  const R Srz = (dz[UR] + dr[UZ]) / K(2.0);
+  const R Szp = r * dz[OMG] / K(2.0);
+  const R Spr = r * dr[OMG] / K(2.0);
+  const R two_nus = K(2.0) * (p_nus + nuSS);
+  t[UR] += two_nus * (Srr * dr[LND] + Srz * dz[LND]);
+  t[UZ] += two_nus * (Srz * dr[LND] + Szz * dz[LND]);
+  t[OMG] += two_nus * (Spr * dr[LND] + Szp * dz[LND]) / r;
+  t[LNE6] += (two_nus * (Srr * Srr + Szz * Szz + Spp * Spp + K(2.0) * (Srz * Srz + Szp * Szp + Spr * Spr)) +
+              p_nub * div_u * div_u) / eng;
+  // velocity-only viscous terms
+  const R tmp1 = (p_nus + nuSS) + p_nu * sphr_2;
+  const R tmp2 = (p_nus + nuSS) / r;
+  t[UR] += tmp1 * lap[UR] + tmp2 * (dr[UR] - c->ur / r);
+  t[UZ] += tmp1 * lap[UZ] + tmp2 * (dr[UZ]);
+  t[OMG] += tmp1 * lap[OMG] + tmp2 * (dr[OMG] * K(3.0));
+  const R mixed = (p_nus + nuSS) / K(3.0) + p_nub;
+  t[UR] += mixed * (drr_ur + drz_uz + (dr[UR] - c->ur / r) / r);
+  t[UZ] += mixed * (drz_ur + dzz_uz + dz[UR] / r);
+  // density diffusion and conduction
+  const R lap_d_d = lap[LND] + dr[LND] * dr[LND] + dz[LND] * dz[LND];
+  const R lap_e_e = lap[LNE6] + dr[LNE6] * dr[LNE6] + dz[LNE6] * dz[LNE6];
+  t[LND] += lap_d_d * p_dd * sphr_2;
+  t[LNE6] += lap_e_e * (p_ed * sphr_2 + p_kappa * gamma1 + p_gamma * nuSS);
+  // radiation force
+  const R kappa = p_ff * den * den * std::pow(temp, K(-3.5));
+  const R chi = p_es * den + kappa;
+  const R d_lner_2 = dr[LNER] * dr[LNER] + dz[LNER] * dz[LNER];
+  const R bigR = std::sqrt(d_lner_2) / chi;
+  const R denom = K(6.0) + (K(3.0) + bigR) * bigR;
+  const R Lambda = (K(2.0) + bigR) / denom;
+  t[UR] -= Lambda * rad * (dr[LND] + dr[LNE6]);
+  t[UZ] -= Lambda * rad * (dz[LND] + dz[LNE6]);
+  // heating / cooling
+  const R temp2 = temp * temp;
+  const R cooling = kappa * (p_ar * temp2 * temp2 / den - rad);
+  t[LNE6] -= cooling / eng;
+  t[LNER] += cooling / rad;
+  // radiation diffusion
+  const R d_lnd_d_lner = dr[LND] * dr[LNER] + dz[LND] * dz[LNER];
+  const R lap_er_er = lap[LNER] + d_lner_2;
+  const R nu_rad = Lambda / chi;
+  const R Lambdap = -bigR * (K(4.0) + bigR) / (denom * denom);
+  const R dr_e = dr[LND] + dr[LNER], dz_e = dz[LND] + dz[LNER];
+  const R drr_e = drr_lnd + drr_lner, drz_e = drz_lnd + drz_lner, dzz_e = dzz_lnd + dzz_lner;
+  const R dr_chi = chi * dr[LND] - K(3.5) * kappa * dr[LNE6];
+  const R dz_chi = chi * dz[LND] - K(3.5) * kappa * dz[LNE6];
+  const R dr_bigR = ((dr_e * drr_e + dz_e * drz_e) / (K(1e-16) + bigR) / chi - bigR * dr_chi) / chi;
+  const R dz_bigR = ((dr_e * drz_e + dz_e * dzz_e) / (K(1e-16) + bigR) / chi - bigR * dz_chi) / chi;
+  t[LNER] += lap_er_er * p_rd * sphr_2 + nu_rad * (lap_d_d + K(2.0) * d_lnd_d_lner + lap_er_er) +
+             dr_e * (Lambdap * dr_bigR - nu_rad * dr_chi) / chi + dz_e * (Lambdap * dz_bigR - nu_rad * dz_chi) / chi;
+  // gravity
+  const R tmp = sphr - p_rS;
+  const R gr = p_M / (tmp * tmp);
+  t[UR] -= sint * gr;
+  t[UZ] -= cost * gr;
+  S out;
+  std::memcpy(&out, t, sizeof(out));
+  return out;
+}
+
+// src/disk/Euler.cuh:19-69: radiation-matter equilibrium where free-free cooling would
+// overshoot it within dt (positive root of x^4 + x - x0 = 0 in closed form).
+void first_order(S *u, R dt, int i, int j)
+{
+  (void)i; (void)j;
+  const R den = std::exp(u->lnd), eng = std::exp(u->lne), rad = std::exp(u->lner);
+  const R gamma1 = p_gamma - K(1.0);
+  const R gamma1_2 = gamma1 * gamma1;
+  const R scale = std::pow(p_ar * gamma1_2 * gamma1_2 / den, K(1.0) / K(3.0));
+  const R x0 = (eng + rad) * scale;
+  const R a = std::pow(std::sqrt(K(0.00390625) + x0 * x0 * x0 / K(27.0)) + K(0.0625), K(1.0) / K(3.0));
+  const R b = a - x0 / (K(3.0) * a);
+  const R cq = std::sqrt(K(2.0) * b);
+  const R eq_eng = (std::sqrt(K(0.5) / cq - K(0.5) * b) - K(0.5) * cq) / scale;
+  const R dt_eng = (eq_eng - eng) / dt;
+  const R temp = gamma1 * eng;
+  const R temp2 = temp * temp;
+  const R kappa = p_ff * den * den * std::pow(temp, K(-3.5));
+  const R cooling = kappa * (p_ar * temp2 * temp2 / den - rad);
+  if (cooling * cooling > dt_eng * dt_eng) {
+    u->lne = std::log(eq_eng);
+    u->lner = std::log(eng + rad - eq_eng);
+  }
+}
+
+// src/disk/bcond.cuh:19-29: u_R flips sign at the poles.
+R transform(int var, R x) { return var == UR ? -x : x; }
 #endif
 
 }  // namespace

@@ -28,8 +28,12 @@
 // the float functions, so the host build must see the float overloads too.
 using std::cos;
 using std::exp;
+using std::log;
+using std::pow;
 using std::sin;
 using std::sqrt;
+// src/disk/eqns.cuh:47 calls sincos on R; the device library has the float overload.
+static inline void sincos(float x, float *s, float *c) { sincosf(x, s, c); }
 
 // src/hydro/bcond.cuh and src/hydro-isot/bcond.cuh select the variable by threadIdx.x.
 static struct { int x, y, z; } threadIdx;
@@ -60,8 +64,13 @@ Key keys[] = {{"gamma", &para_gamma}, {"nus", &para_nus}, {"nub", &para_nub},
 #elif defined(FG2_SCHEME_ISOT)
 Key keys[] = {{"dd", &para_dd}, {"nus", &para_nus}, {"nub", &para_nub},
               {"cs2", &para_cs2}, {"f", &para_f}, {"k", &para_k}};
+#elif defined(FG2_SCHEME_DISK)
+Key keys[] = {{"M", &para_M},         {"rS", &para_rS},   {"rin", &para_rin}, {"gamma", &para_gamma},
+              {"nus", &para_nus},     {"nub", &para_nub}, {"kappa", &para_kappa}, {"alpha", &para_alpha},
+              {"ar", &para_ar},       {"es", &para_es},   {"ff", &para_ff},   {"dd", &para_dd},
+              {"nu", &para_nu},       {"ed", &para_ed},   {"rd", &para_rd}};
 #else
-#error "define FG2_SCHEME_HYDRO or FG2_SCHEME_ISOT"
+#error "define FG2_SCHEME_HYDRO, FG2_SCHEME_ISOT or FG2_SCHEME_DISK"
 #endif
 }  // namespace
 
@@ -134,15 +143,17 @@ void orc_deriv(const R *u, int n1, int n2, int which, int field, R *out)
       const S *u = o + (long)i * sc + j;  // THIS = u, STRIDE = s (src/deriv.h:25-31)
       const int s = sc;
       R r = 0, fld[5][NVAR];
-      fld[0][0] = D1(lnd); fld[0][1] = D1(u1); fld[0][2] = D1(u2);
-      fld[1][0] = D2(lnd); fld[1][1] = D2(u1); fld[1][2] = D2(u2);
-      fld[2][0] = D11(lnd); fld[2][1] = D11(u1); fld[2][2] = D11(u2);
-      fld[3][0] = D22(lnd); fld[3][1] = D22(u1); fld[3][2] = D22(u2);
-      fld[4][0] = D12(lnd); fld[4][1] = D12(u1); fld[4][2] = D12(u2);
+#define ORC_FIELD(k, name) \
+  fld[0][k] = D1(name); fld[1][k] = D2(name); fld[2][k] = D11(name); fld[3][k] = D22(name); fld[4][k] = D12(name);
+#if defined(FG2_SCHEME_DISK)
+      ORC_FIELD(0, lnd) ORC_FIELD(1, ur) ORC_FIELD(2, uz) ORC_FIELD(3, Omg) ORC_FIELD(4, lne) ORC_FIELD(5, lner)
+#else
+      ORC_FIELD(0, lnd) ORC_FIELD(1, u1) ORC_FIELD(2, u2)
 #if defined(FG2_SCHEME_HYDRO)
-      fld[0][3] = D1(lne); fld[1][3] = D2(lne); fld[2][3] = D11(lne); fld[3][3] = D22(lne);
-      fld[4][3] = D12(lne);
+      ORC_FIELD(3, lne)
 #endif
+#endif
+#undef ORC_FIELD
       r = fld[which][field];
       out[(long)i * n2 + j] = r;
     }

@@ -6,6 +6,16 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
+# The reference's parameter defaults per scheme (src/hydro/eqns.cuh:19-24,
+# src/hydro-isot/eqns.cuh:19-25, src/disk/eqns.cuh:19-36).
+DEFAULTS = {
+    "hydro": {"gamma": 5 / 3, "nus": 2e-4, "nub": 0.0, "kappa": 5e-4, "dd": 0.0},
+    "hydro-isot": {"dd": 0.0, "nus": 2e-4, "nub": 0.0, "cs2": 1.0, "f": 0.0, "k": -8.0},
+    "disk": {"M": 1.0, "rS": 2.0, "rin": 3.0, "gamma": 5 / 3, "nus": 0.0, "nub": 0.0, "kappa": 0.0,
+             "alpha": 0.01, "ar": 1.0e8, "es": 1.0, "ff": 0.0, "dd": 1.0e-4, "nu": 2.0e-4, "ed": 5.0e-4,
+             "rd": 5.0e-4},
+}
+
 
 def golden_cases():
     return sorted(os.path.splitext(os.path.basename(p))[0] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))

@@ -47,6 +47,34 @@ def test_scheme_metadata():
     assert i.fg2_scheme_name() == b"hydro-isot" and i.fg2_nvar() == 3 and i.fg2_eqns_flop() == 214
     assert [i.fg2_para_key(k) for k in range(i.fg2_para_count())] == [b"dd", b"nus", b"nub", b"cs2", b"f", b"k"]
     assert h.fg2_field_name(4) is None
+    d = fg2_b200.load_library("disk")
+    assert d.fg2_scheme_name() == b"disk" and d.fg2_nvar() == 6 and d.fg2_eqns_flop() == 733
+    assert [d.fg2_field_name(f) for f in range(6)] == [b"lnd", b"ur", b"uz", b"Omg", b"lne", b"lner"]
+    assert [d.fg2_para_key(k) for k in range(d.fg2_para_count())] == [
+        b"M", b"rS", b"rin", b"gamma", b"nus", b"nub", b"kappa", b"alpha", b"ar", b"es", b"ff", b"dd", b"nu",
+        b"ed", b"rd"]
+
+
+def test_six_field_scheme_refuses_16bit_storage_before_any_device_call():
+    lib = fg2_b200.load_library("disk")
+    for code in (fg2_b200.STORAGE["f16"], fg2_b200.STORAGE["bf16"]):
+        assert not lib.fg2_sim_create(64, 64, code, None)
+        assert b"at most 4 fields" in lib.fg2_last_error()
+
+
+def test_disk_host_setup_is_the_hawley_torus():
+    """src/disk/init.h:31-58 at cell centres (ln(r / r_in), theta) of the scheme's own box."""
+    from oracle.oracle import disk_box
+    n1, n2 = 24, 32
+    l1, l2 = disk_box(n1, n2, f64=True)
+    x, known = fg2_b200.setup_evaluate("Hawley", n1, n2, scheme="disk", l1=l1, l2=l2)
+    assert known and x.shape == (n1, n2, 6)
+    assert np.all(x[..., 1:3] == 0.0) and np.all(x[..., 5] == x[0, 0, 5])
+    assert np.isclose(x[..., 0].min(), np.log(1e-4)) and x[..., 0].max() > np.log(0.5)
+    # pressure maximum of the torus at r0 = 16 on the equator, density d0 = 1 there
+    lnr = l1 * (np.arange(n1) + 0.5) / n1
+    i = int(np.argmin(np.abs(3.0 * np.exp(lnr) - 16.0)))
+    assert abs(x[i, n2 // 2, 0]) < 0.2
 
 
 def test_bad_sizes_rejected_before_any_device_call():

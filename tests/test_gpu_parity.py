@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import fg2_b200
-from helpers import golden_cases, load_golden, rel_l2
+from helpers import DEFAULTS, golden_cases, load_golden, rel_l2
 from oracle.oracle import Oracle, reference_delta, reference_dt
 
 pytestmark = pytest.mark.gpu
@@ -42,9 +42,7 @@ def test_steps_match_golden(name, cuda):
 def f64_kick(g, v_in=None, beta=0.0):
     """The right-hand side in FP64 (the port at R = double) from the same FP32 inputs."""
     o = Oracle(g["scheme"], "f64", "port")
-    defaults = {"hydro": {"gamma": 5 / 3, "nus": 2e-4, "nub": 0.0, "kappa": 5e-4, "dd": 0.0},
-                "hydro-isot": {"dd": 0.0, "nus": 2e-4, "nub": 0.0, "cs2": 1.0, "f": 0.0, "k": -8.0}}[g["scheme"]]
-    for k, v in {**defaults, **g["para"]}.items():
+    for k, v in {**DEFAULTS[g["scheme"]], **g["para"]}.items():
         o.set_para(k, float(np.float32(v)) if g["prec"] == "f32" else v)
     o.set_delta(g["delta1"], g["delta2"])
     u = o.padded(g["x0"].astype(np.float64))

@@ -5,13 +5,8 @@ tests on polynomials and a convergence-order check."""
 import numpy as np
 import pytest
 
-from helpers import golden_cases, load_golden
+from helpers import DEFAULTS, golden_cases, load_golden
 from oracle.oracle import HALO, Oracle, available, reference_delta, reference_dt
-
-DEFAULTS = {
-    "hydro": {"gamma": 5 / 3, "nus": 2e-4, "nub": 0.0, "kappa": 5e-4, "dd": 0.0},
-    "hydro-isot": {"dd": 0.0, "nus": 2e-4, "nub": 0.0, "cs2": 1.0, "f": 0.0, "k": -8.0},
-}
 
 
 def configured(g, kind):
@@ -42,6 +37,10 @@ def test_golden_bit_exact(name, kind):
     v = o.padded(g["v_in"])
     o.kick(v, u, 0.0, -5.0 / 9.0)
     assert np.array_equal(o.interior(v), g["kick1"])
+    if "euler_out" in g:  # the Euler hook alone
+        u = o.padded(g["x0"])
+        o.euler(u, g["dt"])
+        assert np.array_equal(o.interior(u), g["euler_out"])
     # full steps
     u = o.padded(g["x0"])
     v = o.empty(n1, n2)
