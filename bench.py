@@ -264,11 +264,14 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
         m.init("turb", seed=BATCH_SEED * 100000 + k)
     x0 = [m.download() for m in b.members]
     if tiling:
-        b.set_tiling(*tiling)
+        b.set_tiling(*tiling[:2])
+        if len(tiling) > 2:
+            b.set_strip(tiling[2])
         tune_ms = None
     else:
         tune_ms = b.autotune(reps=4)
     nb, ctas = b.tiling()
+    strip = b.strip()
     cells = b.cells
     stream = torch.cuda.ExternalStream(b.stream, device=device)
     b.set_time(0.0)
@@ -290,7 +293,8 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
     result = {"workload": f"{len(sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
                           "box 2 pi, k^-2 random-phase velocity rms Mach 0.3, FP32, per-member CFL dt",
               "cells": cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
-              "status": status, "tiling": {"blocks_of_7_rows": nb, "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
+              "status": status, "tiling": {"strip_columns": strip, "warps_per_cta": strip // 32, "blocks_of_7_rows": nb,
+                         "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
               "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
                            "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
                            "frac": value * B_ALG_ISOT / peak},
@@ -673,7 +677,8 @@ def main():
     ap.add_argument("--no-disk", action="store_true", help="skip the disk-scheme leg")
     ap.add_argument("--only-disk", action="store_true", help="run the disk-scheme leg alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
-    ap.add_argument("--batch-tiling", default="", help="nb,ctas_per_sm for the batch leg (default: autotune)")
+    ap.add_argument("--batch-tiling", default="",
+                    help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
                     help="state storage of the headline workload (f16/bf16: deviation storage)")
     args = ap.parse_args()

@@ -76,6 +76,7 @@ def _bind(lib):
         "fg2_batch_set_time": (I, [P, D]), "fg2_batch_advance": (I, [P, I, D, D, I]),
         "fg2_batch_sync": (I, [P]), "fg2_batch_set_tiling": (I, [P, I, I]),
         "fg2_batch_get_tiling": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "fg2_batch_set_strip": (I, [P, I]), "fg2_batch_get_strip": (I, [P]),
         "fg2_batch_autotune": (I, [P, I, ctypes.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
@@ -391,6 +392,13 @@ class Batch:
         nb, c = ctypes.c_int(), ctypes.c_int()
         self._check(self.lib.fg2_batch_get_tiling(self.h, ctypes.byref(nb), ctypes.byref(c)), "tiling")
         return nb.value, c.value
+
+    def set_strip(self, width):
+        """Strip width of the batch launches: 64 or 128 columns per tile (2 or 4 warps per CTA)."""
+        self._check(self.lib.fg2_batch_set_strip(self.h, int(width)), "set_strip")
+
+    def strip(self):
+        return self.lib.fg2_batch_get_strip(self.h)
 
     def autotune(self, reps=3):
         ms = ctypes.c_double()

@@ -50,16 +50,16 @@ struct fg2_batch {
   // what the descriptors were built for
   bool desc_valid = false;
   bool desc_device_dt = false;
-  int desc_nb = 0;
+  int desc_nb = 0, desc_strip = 0;
   std::vector<unsigned> versions;
   std::vector<int> curs;
   // tiling (autotuned or set)
-  int nb = TILE_BLOCKS_DEFAULT, max_ctas = 0;
+  int nb = TILE_BLOCKS_DEFAULT, max_ctas = 0, strip = STRIP_DEFAULT;
   int reverse = 0;  // tile order of the next substage launch (alternates)
   // the two-step graph and what it was captured for
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0, graph_tend = 0;
-  int graph_nb = 0, graph_ctas = 0;
+  int graph_nb = 0, graph_ctas = 0, graph_strip = 0;
   std::vector<double> graph_para;
 };
 
@@ -87,7 +87,7 @@ int check_members(fg2_batch *b)
 // Descriptor sets for the members' current parities, tile order and dt mode.
 int ensure_batch_descs(fg2_batch *b, bool device_dt)
 {
-  bool valid = b->desc_valid && b->desc_device_dt == device_dt && b->desc_nb == b->nb;
+  bool valid = b->desc_valid && b->desc_device_dt == device_dt && b->desc_nb == b->nb && b->desc_strip == b->strip;
   for (int k = 0; valid && k < b->count; ++k)
     valid = b->versions[k] == b->members[k]->version && b->curs[k] == b->members[k]->cur;
   if (valid) return FG2_OK;
@@ -99,10 +99,11 @@ int ensure_batch_descs(fg2_batch *b, bool device_dt)
     for (int set = 0; set < 2; ++set) {
       const int in = set == 0 ? m->cur : 1 - m->cur;
       if (make_grid_desc(&b->desc_host[(size_t)set * b->count + r], m->u[in], m->u[1 - in], m->v, m->L, m->storage,
-                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0, dev_code(m)) != CUDA_SUCCESS)
+                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0, dev_code(m),
+                         b->strip) != CUDA_SUCCESS)
         return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed for batch member %d", k);
     }
-    tile0 += substage_tiles(m->L, b->nb);
+    tile0 += substage_tiles(m->L, b->nb, b->strip);
     b->limits_host[k] = make_double2(m->c, diffusive_dt(m));
     b->versions[k] = m->version;
     b->curs[k] = m->cur;
@@ -114,6 +115,7 @@ int ensure_batch_descs(fg2_batch *b, bool device_dt)
   b->desc_valid = true;
   b->desc_device_dt = device_dt;
   b->desc_nb = b->nb;
+  b->desc_strip = b->strip;
   return FG2_OK;
 }
 
@@ -137,6 +139,7 @@ int enqueue_batch_step(fg2_batch *b, double dt, bool device_dt, double t_end, in
     a.status = b->status;
     a.nb = b->nb;
     a.max_ctas = b->max_ctas;
+    a.strip = b->strip;
     a.reverse = b->reverse;
     b->reverse ^= 1;
     a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
@@ -395,6 +398,16 @@ int fg2_batch_get_tiling(const fg2_batch *b, int *nb, int *ctas_per_sm)
   return FG2_OK;
 }
 
+int fg2_batch_set_strip(fg2_batch *b, int width)
+{
+  if (!b || (width != 64 && width != 128)) return fail(FG2_ERR_ARG, "strip width must be 64 or 128, not %d", width);
+  if (width != b->strip) drop_batch_graph(b);
+  b->strip = width;
+  return FG2_OK;
+}
+
+int fg2_batch_get_strip(const fg2_batch *b) { return b ? b->strip : -1; }
+
 int fg2_batch_advance(fg2_batch *b, int nsteps, double dt, double t_end, int use_graph)
 {
   if (!b || nsteps < 0) return fail(FG2_ERR_ARG, "bad arguments");
@@ -413,7 +426,7 @@ int fg2_batch_advance(fg2_batch *b, int nsteps, double dt, double t_end, int use
   if (rc) return rc;
   const std::vector<double> para(b->members[0]->para, b->members[0]->para + NPARA);
   if (b->graph && (b->graph_dt != dt || b->graph_tend != t_end || b->graph_nb != b->nb || b->graph_ctas != b->max_ctas ||
-                   b->graph_para != para))
+                   b->graph_strip != b->strip || b->graph_para != para))
     drop_batch_graph(b);
   if (!b->graph) {
     // two steps = six substages: the descriptor set returns to the start
@@ -435,6 +448,7 @@ int fg2_batch_advance(fg2_batch *b, int nsteps, double dt, double t_end, int use
     b->graph_tend = t_end;
     b->graph_nb = b->nb;
     b->graph_ctas = b->max_ctas;
+    b->graph_strip = b->strip;
     b->graph_para = para;
   }
   for (int n = 0; n + 1 < nsteps; n += 2) CK(cudaGraphLaunch(b->graph, b->stream));
@@ -468,19 +482,23 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   int rc = check_members(b);
   if (rc) return rc;
   struct Cand {
-    int nb, ctas;
+    int strip, nb, ctas;
     double ms;
   };
   std::vector<Cand> cands;
-  // CTAs per SM: 0 = as many as fit (the occupancy limit), or capped at 1, 2 or 3
-  for (int nb : {2, 3, 4, 5, 6, 8})
-    for (int ctas : {0, 1, 2, 3}) cands.push_back({nb, ctas, std::numeric_limits<double>::infinity()});
-  const int keep_nb = b->nb, keep_ctas = b->max_ctas;
+  // strip width 128 or 64 columns (4 or 2 warps per CTA); tile height nb blocks of 7 rows;
+  // CTAs per SM: 0 = as many as fit (the occupancy limit), or capped at 4, 8 or 12 warps
+  for (int strip : {128, 64})
+    for (int nb : {2, 3, 4, 5, 6, 8})
+      for (int warps : {0, 4, 8, 12})
+        cands.push_back({strip, nb, warps * 32 / strip, std::numeric_limits<double>::infinity()});
+  const int keep_nb = b->nb, keep_ctas = b->max_ctas, keep_strip = b->strip;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   rc = prepare_members(b, false);
   auto measure = [&](Cand &c) -> int {
+    b->strip = c.strip;
     b->nb = c.nb;
     b->max_ctas = c.ctas;
     int r = ensure_batch_descs(b, false);
@@ -506,6 +524,7 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  b->strip = rc ? keep_strip : cands[0].strip;
   b->nb = rc ? keep_nb : cands[0].nb;
   b->max_ctas = rc ? keep_ctas : cands[0].ctas;
   drop_batch_graph(b);

@@ -91,6 +91,7 @@ struct KParams {
   const double *dt_dev;  // device time step for grids without their own, or null: dt
   Status *status;        // launch errors
   int nb;                // output blocks of 7 rows per tile
+  int strip;             // strip width (columns per tile, threads per CTA)
   int reverse;           // tiles last first
   unsigned wait_test_bytes;  // extra bytes every chunk expects (timeout-path tests; 0 otherwise)
   double comp_bg;        // beta * gamma of the next stage (16-bit residual carry), or 0
@@ -148,6 +149,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.dt_dev = a.dt_dev;
   kp.status = a.status;
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
+  kp.strip = strip_width(a.strip);
   kp.comp_bg = a.comp_bg;
   kp.reverse = a.reverse;
   kp.wait_test_bytes = a.wait_test_bytes;
@@ -261,18 +263,19 @@ CUresult encode_map(CUtensorMap *map, const void *base, const Layout &L, int sto
 
 CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
                         int p2, double delta1, double delta2, const double *dt, Status *status, int tile0,
-                        const DevCode *dev)
+                        const DevCode *dev, int strip)
 {
-  CUresult r = encode_map(&d->tm_u, u_in, L, storage, sub::BW, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+  const int sw = strip_width(strip);
+  CUresult r = encode_map(&d->tm_u, u_in, L, storage, sw + 2 * GL, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
   // the v box starts GL % G cells left of the strip when a cell group is wider than GL
-  const int G = group_cells(storage), vbw = (sub::SW + GL % G + G - 1) / G * G;
+  const int G = group_cells(storage), vbw = (sw + GL % G + G - 1) / G * G;
   r = encode_map(&d->tm_v, v, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
   d->u_out = u_out;
   d->v = v;
   d->L = L;
-  d->strips = sub::tile_grid(L, sub::NB_DEFAULT).strips;
+  d->strips = sub::tile_grid(L, sub::NB_DEFAULT, sw).strips;
   d->tile0 = tile0;
   d->p1 = p1;
   d->p2 = p2;
@@ -290,14 +293,19 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   return CUDA_SUCCESS;
 }
 
-int substage_tiles(const Layout &L, int nb) { return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT).ntiles; }
+int strip_width(int strip) { return strip == 64 ? 64 : STRIP_DEFAULT; }
 
-template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
-static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
-                                int max_ctas, int *queue, cudaStream_t s)
+int substage_tiles(const Layout &L, int nb, int strip)
 {
-  using G = sub::Geo<S, RV>;
-  auto kern = sub::substage_kernel<S, M2, RV, WV, WU, CF, SC>;
+  return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT, strip_width(strip)).ntiles;
+}
+
+template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC, int W>
+static cudaError_t run_substage_w(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
+                                  int max_ctas, int *queue, cudaStream_t s)
+{
+  using G = sub::Geo<S, RV, W>;
+  auto kern = sub::substage_kernel<S, M2, RV, WV, WU, CF, SC, W>;
   static int ctas_per_sm = 0, sms = 0;
   if (!ctas_per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
@@ -305,15 +313,28 @@ static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, c
     int dev = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, sub::NT, G::SMEM)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, W, G::SMEM)) != cudaSuccess)
       return e;
     if (ctas_per_sm < 1) return cudaErrorInvalidConfiguration;
   }
   if (ntiles < 1) return cudaSuccess;
   int grid = sms * (max_ctas > 0 && max_ctas < ctas_per_sm ? max_ctas : ctas_per_sm);
   if (grid > ntiles) grid = ntiles;
-  kern<<<grid, sub::NT, G::SMEM, s>>>(grids, ngrids, ntiles, kp, queue);
+  kern<<<grid, W, G::SMEM, s>>>(grids, ngrids, ntiles, kp, queue);
   return cudaGetLastError();
+}
+
+// Single grids use the default strip; batch launches (SC) may take the narrower one.
+template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC>
+static cudaError_t run_substage(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
+                                int max_ctas, int *queue, cudaStream_t s)
+{
+  if constexpr (SC) {
+    if (kp.strip == 64) return run_substage_w<S, M2, RV, WV, WU, CF, SC, 64>(grids, ngrids, ntiles, kp, max_ctas, queue, s);
+  } else {
+    if (kp.strip == 64) return cudaErrorInvalidValue;
+  }
+  return run_substage_w<S, M2, RV, WV, WU, CF, SC, STRIP_DEFAULT>(grids, ngrids, ntiles, kp, max_ctas, queue, s);
 }
 
 template <class S, unsigned M2, bool SC>

@@ -26,6 +26,8 @@ struct StageArgs {
   Status *status;       // device status block (launch errors; per-grid blocks are in GridDesc)
   int nb = 0;           // tile height in blocks of 7 rows (0: the default)
   int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
+  int strip = 0;        // strip width: 64 or 128 columns per tile (0: 128); one thread per
+                        // column, so 2 or 4 warps per CTA; the descriptors must match it
   double comp_bg = 0;   // beta * gamma of the next stage: 16-bit state carries its rounding
                         // residual into that stage through v (0: no next stage)
   int reverse = 0;      // take the tiles last first (alternated from launch to launch, so a
@@ -63,13 +65,17 @@ struct GridDesc {
 
 // Fills a GridDesc (tensor maps over u_in and v encoded here).  Returns CUDA_SUCCESS or the
 // driver's error.
+// `strip` is the strip width the descriptors are for (box widths and tiles per row; 0: 128).
 CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, const Layout &L, int storage, int p1,
                         int p2, double delta1, double delta2, const double *dt, Status *status, int tile0,
-                        const DevCode *dev = nullptr);
+                        const DevCode *dev = nullptr, int strip = 0);
 // Tile height of the substage kernel in blocks of 7 output rows, unless a launch sets nb.
 constexpr int TILE_BLOCKS_DEFAULT = 5;
-// Tiles of one grid for a tile height of nb blocks of 7 rows (0: the default).
-int substage_tiles(const Layout &L, int nb = 0);
+// Strip width of single-grid launches; batch launches may also use 64 (strip_width(64)).
+constexpr int STRIP_DEFAULT = 128;
+int strip_width(int strip);
+// Tiles of one grid for a tile height of nb blocks of 7 rows and a strip width (0: defaults).
+int substage_tiles(const Layout &L, int nb = 0, int strip = 0);
 
 // One fused substage over the grids of `grids` (device array of ngrids descriptors holding
 // ntiles tiles in all).  `scaled`: the grids differ in Delta (stencil weights scaled per grid);

@@ -2,12 +2,12 @@
 // by kernels.cu, once per scheme).
 //
 // Work decomposition.  A launch advances a list of grids (one simulation, or a batch of
-// independent simulations of any sizes).  A tile is a strip of SW = 128 interior columns by
-// 7 nb rows of one grid (nb blocks of 7 output rows, a launch parameter, 5 by default); the
-// launch's tiles are numbered grid by grid, strip fastest, and a persistent grid of CTAs
-// drains them from a queue (an atomic counter that the last CTA to finish resets, so a launch
-// needs no host-side reset and replays from a CUDA graph).  A CTA
-// has 4 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in
+// independent simulations of any sizes).  A tile is a strip of W interior columns (128, or
+// 64 in batch launches) by 7 nb rows of one grid (nb blocks of 7 output rows, a launch
+// parameter, 5 by default); the launch's tiles are numbered grid by grid, strip fastest, and
+// a persistent grid of CTAs drains them from a queue (an atomic counter that the last CTA to
+// finish resets, so a launch needs no host-side reset and replays from a CUDA graph).  A CTA
+// has W / 32 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in
 // device memory: its TMA tensor maps, output pointers, layout, boundaries, time step and
 // status block.
 //
@@ -55,18 +55,19 @@ namespace sub {
 #ifndef FG2_NSLOT
 #define FG2_NSLOT 2
 #endif
-#ifndef FG2_SW
-#define FG2_SW 128
-#endif
-
-constexpr int SW = FG2_SW;         // interior columns per tile (strip width)
-constexpr int BW = SW + 2 * GL;    // TMA box width of u (halo 4 + 4; the stencil uses 3)
 constexpr int CH = 7;              // rows per chunk = register window period
 constexpr int NB_DEFAULT = TILE_BLOCKS_DEFAULT;  // output blocks per tile unless a launch sets nb
-constexpr int NCW = SW / 32;       // warps per CTA
-constexpr int NT = NCW * 32;       // threads per CTA, one per strip column
 constexpr int NP = (NV + 1) / 2;   // field pairs
-static_assert(NT == SW, "one thread per strip column");
+
+// Strip geometry of a launch: W interior columns per tile, one thread per column (W / 32
+// warps per CTA), and the TMA box of u W + 8 columns wide (halo 4 + 4; the stencil uses 3).
+template <int W>
+struct Strip {
+  static constexpr int SW = W;
+  static constexpr int BW = W + 2 * GL;
+  static constexpr int NT = W;
+  static_assert(W % 32 == 0 && W >= 32 && W <= 256, "whole warps, at most 8 per CTA");
+};
 
 // Fields with a mixed derivative D12 (the scheme's D12_FIELDS), in field order: the k-th of
 // them has streaming accumulator k.
@@ -89,8 +90,9 @@ __host__ __device__ constexpr int group_of(int elem)
 // reads v), the FP32 copy of the landed u box (deviation storage), then the mbarriers and
 // the producer's bookkeeping.  The v box starts VOFF cells left of the strip when a cell
 // group is wider than the 4 ghost columns.
-template <class S, bool RV>
+template <class S, bool RV, int W>
 struct Geo {
+  static constexpr int SW = Strip<W>::SW, BW = Strip<W>::BW;
   static constexpr bool DEV = Store<S>::DEV;
   static constexpr int NSLOT = FG2_NSLOT;
   static constexpr int CB = NV * (int)sizeof(S);  // bytes per cell
@@ -235,11 +237,11 @@ struct TileGrid {
   int strips, rows, ntiles;
 };
 
-__host__ __device__ inline TileGrid tile_grid(const Layout &L, int nb)
+__host__ __device__ inline TileGrid tile_grid(const Layout &L, int nb, int sw)
 {
   TileGrid g;
   const int th = nb * CH;
-  g.strips = (L.n2 + SW - 1) / SW;
+  g.strips = (L.n2 + sw - 1) / sw;
   g.rows = (L.n1 + th - 1) / th;
   g.ntiles = g.strips * g.rows;
   return g;
@@ -595,12 +597,12 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 }
 
 // Issues the next chunk of the CTA's sequence into its slot (free by the caller's check).
-template <class S, bool READ_V>
+template <class S, bool READ_V, int W>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
                                             bool reverse, unsigned extra_bytes, int *queue)
 {
-  using G = Geo<S, READ_V>;
+  using G = Geo<S, READ_V, W>;
   if (ps->done) return;
   const int n = ps->next_n, s = n % G::NSLOT;
   if (ps->c == 0) {
@@ -614,7 +616,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
       const int local = t - grids[g].tile0, strips = grids[g].strips;
       ps->g = g;
       ps->i0 = (local / strips) * (nb * CH);
-      ps->j0 = (local % strips) * SW;
+      ps->j0 = (local % strips) * W;
       grid_of[s] = g;
     }
   }
@@ -682,7 +684,7 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
 // rows prow0 .., box column 0 = padded column j0) into FP32 cells dec ([row][ncol][NV]):
 // bg + s h with s of the tile of the interior cell each value images.  This thread takes
 // every step-th column from `first`.
-template <class S>
+template <class S, int BOXW>
 __device__ __forceinline__ void decode_cols(const S *box, float *dec, int ncol, int c0, int first, int step, int prow0,
                                             int j0, const GridRegs<S> &gr)
 {
@@ -699,7 +701,7 @@ __device__ __forceinline__ void decode_cols(const S *box, float *dec, int ncol, 
       const float4 sc = __ldg(gr.scale + ti * gr.tiles2 + tj);
       const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
       float2 h[NP];
-      load_cell<S>(box + (r * BW + cc) * NV, h);
+      load_cell<S>(box + (r * BOXW + cc) * NV, h);
 #pragma unroll
       for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
       st_cell<float>(dec + (r * ncol + c) * NV, h);
@@ -725,13 +727,14 @@ __device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
   rate = T(0);
 }
 
-template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? (NV > 4 ? 2 : 3) : 1) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
+template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC, int W>
+__global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4 ? 2 : 3) * (128 / W) : 128 / W) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
                                                          const KParams<typename Store<S>::C> a, int *queue)
 {
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
-  using G = Geo<S, READ_V>;
+  using G = Geo<S, READ_V, W>;
+  constexpr int SW = Strip<W>::SW, BW = Strip<W>::BW, NT = Strip<W>::NT;
   constexpr bool DEV = Store<S>::DEV;
   constexpr int NS = G::NSLOT;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -748,7 +751,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? (NV > 
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);
+    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);
   }
   __syncthreads();
 
@@ -797,7 +800,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? (NV > 
       prow0 = i0 + CH * b + 3 + GT;
     }
     if constexpr (DEV) {
-      decode_cols<S>(sbox, dec, BW, 0, tx, NT, prow0, j0, gr);
+      decode_cols<S, BW>(sbox, dec, BW, 0, tx, NT, prow0, j0, gr);
       __syncthreads();
     }
     if (b < 0) {
@@ -828,7 +831,7 @@ __global__ void __launch_bounds__(NT, sizeof(typename Store<S>::C) == 4 ? (NV > 
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<S, READ_V>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);  // refill slot s
+      issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }

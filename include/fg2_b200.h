@@ -173,11 +173,16 @@ int fg2_batch_set_time(fg2_batch *b, double t);
  * CFL step, device-resident, capped at t_end.  use_graph: replay two captured steps. */
 int fg2_batch_advance(fg2_batch *b, int nsteps, double dt, double t_end, int use_graph);
 int fg2_batch_sync(fg2_batch *b); /* wait; worst status over the members */
-/* Tiling of the batch launches: tile height in blocks of 7 rows (nb) and CTAs per SM
- * (0: as many as fit).  fg2_batch_autotune times steps of each candidate on the batch's own
- * members (with dt = 0, which leaves every state unchanged) and keeps the fastest. */
+/* Tiling of the batch launches: tile height in blocks of 7 rows (nb), CTAs per SM
+ * (0: as many as fit) and strip width (64 or 128 columns per tile, one thread per column:
+ * 2 or 4 warps per CTA; default 128).  fg2_batch_autotune times steps of each candidate
+ * (strip width x tile height x occupancy cap) on the batch's own members (with dt = 0, which
+ * leaves every state unchanged) and keeps the fastest; the successor of the reference's
+ * block-size heuristic (src/setup.cpp:39-58). */
 int fg2_batch_set_tiling(fg2_batch *b, int nb, int ctas_per_sm);
 int fg2_batch_get_tiling(const fg2_batch *b, int *nb, int *ctas_per_sm);
+int fg2_batch_set_strip(fg2_batch *b, int width);
+int fg2_batch_get_strip(const fg2_batch *b); /* 64 or 128 */
 int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms);
 
 /* ---- allocation-free sums ---------------------------------------------------------------

@@ -136,14 +136,15 @@ def test_member_matches_cpu_port(cuda):
 
 
 def test_tiling_does_not_change_results(cuda):
-    """Every tile height and CTA count gives bitwise the same state (each cell's arithmetic,
-    the order of its sums included, does not depend on the tiling)."""
+    """Every strip width, tile height and CTA count gives bitwise the same state (each cell's
+    arithmetic, the order of its sums included, does not depend on the tiling)."""
     outs = []
-    for nb, ctas in [(5, 0), (2, 1), (8, 2), (3, 3)]:
+    for strip, nb, ctas in [(128, 5, 0), (128, 2, 1), (64, 8, 2), (128, 3, 3), (64, 3, 0), (64, 5, 6)]:
         b, alone = make_pair("hydro", SIZES[:4], "noise")
         try:
+            b.set_strip(strip)
             b.set_tiling(nb, ctas)
-            assert b.tiling() == (nb, ctas)
+            assert b.tiling() == (nb, ctas) and b.strip() == strip
             assert b.advance(4, 1e-4, graph=True) == 0
             assert b.sync() == 0
             outs.append([m.download() for m in b.members])
@@ -161,12 +162,39 @@ def test_autotune_keeps_state(cuda):
         ms = b.autotune(reps=2)
         assert ms > 0
         nb, ctas = b.tiling()
-        assert 2 <= nb <= 8 and 0 <= ctas <= 3
+        assert b.strip() in (64, 128)
+        assert 2 <= nb <= 8 and 0 <= ctas <= 12 * 32 // b.strip()
         for a, m in zip(before, b.members):
             assert np.array_equal(a, m.download())
         assert b.advance(2, 1e-3) == 0 and b.sync() == 0
     finally:
         close(b, alone)
+
+
+@pytest.mark.parametrize("storage", ["f16", "f64"])
+def test_strip_width_does_not_change_results_of_other_storages(storage, cuda):
+    """The 64-column strip with 16-bit deviation storage (its decode pass reads the narrower
+    box) and with FP64 cells, bitwise against the default strip."""
+    sizes = [(64, 64), (37, 130), (96, 40)]
+    outs = []
+    for strip in (128, 64):
+        with fg2_b200.Batch(sizes, scheme="hydro", storage=storage) as b:
+            b.config()
+            for k, m in enumerate(b.members):
+                m.init("noise", seed=200 + k)
+            b.set_strip(strip)
+            assert b.advance(4, 1e-4, graph=True) == 0
+            assert b.sync() == 0
+            outs.append([m.download() for m in b.members])
+    for a, c in zip(*outs):
+        assert np.array_equal(a, c)
+
+
+def test_bad_strip_width_is_refused(cuda):
+    with fg2_b200.Batch([(32, 32)], scheme="hydro") as b:
+        with pytest.raises(fg2_b200.FG2Error):
+            b.set_strip(96)
+        assert b.strip() == 128
 
 
 def test_nan_in_one_member_is_reported(cuda):
