@@ -204,9 +204,10 @@ __device__ __noinline__ void store_ghosts(T *u, const Layout L, int i, int j, co
 // CFL signal rate of a cell (the scheme's: (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2 on a
 // Cartesian grid, from the cell's position on a curvilinear one).
 template <class C>
-__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2, int i, int j, C d1, C d2)
+__device__ __forceinline__ C cfl_rate(const C q[NV], const Para<C> &p, C inv1, C inv2, int i, int j, C d1, C d2,
+                                      const scheme::Geom<C> &cg)
 {
-  return scheme::signal_rate<C>(q, p, inv1, inv2, i, j, d1, d2);
+  return scheme::signal_rate<C>(q, p, inv1, inv2, i, j, d1, d2, cg);
 }
 
 // 16-bit deviation storage codes hold at most DEV_MAX_FIELDS fields per cell; kernels for
@@ -495,7 +496,7 @@ __global__ void signal_max_kernel(const T *u, const Layout L, const Para<double>
 #pragma unroll
     for (int f = 0; f < NV; ++f) q[f] = value_at<T>(u, L, dc, f, i, j);
     if constexpr (scheme::CURVILINEAR) {
-      m = fmax(m, scheme::signal_rate<double>(q, p, inv1, inv2, i, j, d1, d2));
+      m = fmax(m, scheme::signal_rate<double>(q, p, inv1, inv2, i, j, d1, d2, scheme::column_geom<double>(j, d2)));
     } else {
       const double cs = scheme::sound_speed<double>(q, p);
       m = fmax(m, (fabs(q[scheme::U1]) + cs) * inv1 + (fabs(q[scheme::U2]) + cs) * inv2);

@@ -9,7 +9,9 @@
 // The gradient in cylindrical (R, z) components is the rotation of the coordinate gradient by
 // theta divided by r, the second derivatives follow from the same rotation plus its
 // curvature terms.  Evaluated in the state precision C (float or double), one cell at a time;
-// exp, sin/cos, sqrt and pow are the accurate library functions.
+// exp, sin/cos, sqrt and pow are the accurate library functions, reciprocals the hardware's
+// (about one ulp in FP32).  sin and cos of the column's angle come from a per-column Geom that
+// the kernel computes once per tile.
 #pragma once
 
 #include <cmath>
@@ -22,18 +24,19 @@ namespace scheme {
 // derived from them on the host.
 enum Slot { MASS = 0, RS = 1, RIN = 2, GAMMA = 3, NUS = 4, NUB = 5, KAPPA = 6, ALPHA = 7, AR = 8,
             ES = 9, FF = 10, DD = 11, NU = 12, ED = 13, RD = 14, NSLOT = 15,
-            GM1 = 15, CSG = 16 };
+            GM1 = 15, CSG = 16, IMASS = 17 };
 constexpr fg2::ParaKey PARA_KEYS[NSLOT] = {
     {"M", MASS, 1.0},        {"rS", RS, 2.0},        {"rin", RIN, 3.0},     {"gamma", GAMMA, 5.0 / 3.0},
     {"nus", NUS, 0.0},       {"nub", NUB, 0.0},      {"kappa", KAPPA, 0.0}, {"alpha", ALPHA, 0.01},
     {"ar", AR, 1.0e+8},      {"es", ES, 1.0},        {"ff", FF, 0.0},       {"dd", DD, 1.0e-4},
     {"nu", NU, 2.0e-4},      {"ed", ED, 5.0e-4},     {"rd", RD, 5.0e-4}};
 
-// gamma - 1 and sqrt(gamma (gamma - 1)) (adiabatic sound speed factor)
+// gamma - 1, sqrt(gamma (gamma - 1)) (adiabatic sound speed factor), 1 / M
 inline void derive(double *v)
 {
   v[GM1] = v[GAMMA] - 1.0;
   v[CSG] = std::sqrt(v[GAMMA] * (v[GAMMA] - 1.0));
+  v[IMASS] = 1.0 / v[MASS];
 }
 
 // Every field carries D11 and D22 (the Laplacians of all six enter), and the mixed
@@ -55,7 +58,27 @@ FG2_HD float pw(float x, float y) { return powf(x, y); }
 FG2_HD double pw(double x, double y) { return pow(x, y); }
 FG2_HD void sc(float x, float *s, float *c) { sincosf(x, s, c); }
 FG2_HD void sc(double x, double *s, double *c) { sincos(x, s, c); }
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+#else
+inline float rcp(float x) { return 1.0f / x; }
+#endif
+FG2_HD double rcp(double x) { return 1.0 / x; }
 }  // namespace m
+
+// The column's angle theta = (j + 1/2) Delta2: its sine, cosine and 1 / sine.
+template <class C>
+struct Geom {
+  C sint, cost, isint;
+};
+template <class C>
+FG2_HD Geom<C> column_geom(int j, C delta2)
+{
+  Geom<C> g;
+  m::sc(((C)j + C(0.5)) * delta2, &g.sint, &g.cost);
+  g.isint = C(1) / g.sint;
+  return g;
+}
 
 // Spherical radius of row i: r_in exp((i + 1/2) Delta1) (src/disk/eqns.cuh:51).
 template <class C>
@@ -63,22 +86,23 @@ FG2_HD C sphr_of(int i, C rin, C delta1) { return rin * m::ex(((C)i + C(0.5)) * 
 
 // dq/dt at cell (i, j).  M2 is unused: every field's D11/D22 is evaluated.
 template <unsigned M2, class C>
-FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2)
+FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2,
+                 const Geom<C> &g)
 {
   using fg2::fmac;
-  C sint, cost;
-  m::sc(((C)j + C(0.5)) * delta2, &sint, &cost);
+  (void)j; (void)delta2;
+  const C sint = g.sint, cost = g.cost;
   const C sphr = sphr_of<C>(i, p.v[RIN], delta1);
-  const C isp = C(1) / sphr;
+  const C isp = m::rcp(sphr);
   const C rc = sphr * sint;  // cylindrical radius
-  const C irc = C(1) / rc;
+  const C irc = isp * g.isint;
   const C sp2 = sphr * sphr;
   const C isp2 = isp * isp;
 
   const C den = m::ex(c.q[LND]), eng = m::ex(c.q[LNE]), rad = m::ex(c.q[LNER]);
   const C g1 = p.v[GM1];
   const C temp = g1 * eng;
-  const C nuss = p.v[ALPHA] * p.v[GAMMA] * temp * rc * m::sq(rc / p.v[MASS]);  // Shakura-Sunyaev
+  const C nuss = p.v[ALPHA] * p.v[GAMMA] * temp * rc * m::sq(rc * p.v[IMASS]);  // Shakura-Sunyaev
 
   // gradient in (R, z): the (ln r, theta) gradient rotated by theta, over r
   const C sr = sint * isp, cr = cost * isp;
@@ -128,7 +152,7 @@ FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int 
   t[UZ] = fmac(two_nus, fmac(srz, dr[LND], szz * dz[LND]), t[UZ]);
   t[OMG] = fmac(two_nus * fmac(spr, dr[LND], szp * dz[LND]), irc, t[OMG]);
   const C shear2 = fmac(srr, srr, fmac(szz, szz, spp * spp)) + C(2) * fmac(srz, srz, fmac(szp, szp, spr * spr));
-  const C ieng = C(1) / eng;
+  const C ieng = m::rcp(eng);
   t[LNE] = fmac(fmac(two_nus, shear2, p.v[NUB] * div * div), ieng, t[LNE]);
 
   // viscous stress divergence (velocity-only terms)
@@ -152,20 +176,20 @@ FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int 
   // free-free opacity only when ff != 0, since 0 * pow(...) is 0 for every physical state
   const C kap = p.v[FF] != C(0) ? p.v[FF] * den * den * m::pw(temp, C(-3.5)) : C(0);
   const C chi = fmac(p.v[ES], den, kap);
-  const C ichi = C(1) / chi;
+  const C ichi = m::rcp(chi);
   const C d_lner_2 = fmac(dr[LNER], dr[LNER], dz[LNER] * dz[LNER]);
   const C bigR = m::sq(d_lner_2) * ichi;
   const C denom = fmac(C(3) + bigR, bigR, C(6));
-  const C idenom = C(1) / denom;
+  const C idenom = m::rcp(denom);
   const C Lambda = (C(2) + bigR) * idenom;
   t[UR] = fmac(-Lambda * rad, dr[LND] + dr[LNE], t[UR]);
   t[UZ] = fmac(-Lambda * rad, dz[LND] + dz[LNE], t[UZ]);
 
   // radiative heating / cooling
   const C temp2 = temp * temp;
-  const C cooling = kap * (p.v[AR] * temp2 * temp2 / den - rad);
+  const C cooling = kap * fmac(p.v[AR] * temp2 * temp2, m::rcp(den), -rad);
   t[LNE] = fmac(-cooling, ieng, t[LNE]);
-  t[LNER] = fmac(cooling, C(1) / rad, t[LNER]);
+  t[LNER] = fmac(cooling, m::rcp(rad), t[LNER]);
 
   // radiation diffusion
   const C d_lnd_d_lner = fmac(dr[LND], dr[LNER], dz[LND] * dz[LNER]);
@@ -176,7 +200,7 @@ FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int 
   const C drr_e = drr_lnd + drr_lner, drz_e = drz_lnd + drz_lner, dzz_e = dzz_lnd + dzz_lner;
   const C dr_chi = fmac(chi, dr[LND], C(-3.5) * kap * dr[LNE]);
   const C dz_chi = fmac(chi, dz[LND], C(-3.5) * kap * dz[LNE]);
-  const C iR = C(1) / (C(1e-16) + bigR);
+  const C iR = m::rcp(C(1e-16) + bigR);
   const C dr_bigR = (fmac(dr_e, drr_e, dz_e * drz_e) * iR * ichi - bigR * dr_chi) * ichi;
   const C dz_bigR = (fmac(dr_e, drz_e, dz_e * dzz_e) * iR * ichi - bigR * dz_chi) * ichi;
   C er = lap_er_er * p.v[RD] * sp2;
@@ -187,7 +211,7 @@ FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int 
 
   // gravity of the central mass, pseudo-Newtonian M / (r - r_S)^2
   const C gd = sphr - p.v[RS];
-  const C gr = p.v[MASS] / (gd * gd);
+  const C gr = p.v[MASS] * m::rcp(gd * gd);
   t[UR] = fmac(-sint, gr, t[UR]);
   t[UZ] = fmac(-cost, gr, t[UZ]);
 
@@ -206,10 +230,11 @@ FG2_HD C sound_speed(const C q[NVAR], const fg2::Para<C> &p)
 // (spherical r and theta, from the cylindrical u_R, u_z) plus the adiabatic sound speed,
 // over the physical cell sizes r Delta1 and r Delta2.
 template <class C>
-FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2)
+FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2,
+                     const Geom<C> &g)
 {
-  C sint, cost;
-  m::sc(((C)j + C(0.5)) * delta2, &sint, &cost);
+  (void)j; (void)delta2;
+  const C sint = g.sint, cost = g.cost;
   const C sphr = sphr_of<C>(i, p.v[RIN], delta1);
   const C cs = sound_speed<C>(q, p);
   using fg2::fmac;

@@ -34,9 +34,20 @@ inline unsigned d2_fields(const double *v)
   return m;
 }
 
+// Per-column geometry of a cell (none on the Cartesian grid).
+template <class C>
+struct Geom {};
+template <class C>
+FG2_HD Geom<C> column_geom(int j, C delta2)
+{
+  (void)j; (void)delta2;
+  return Geom<C>{};
+}
+
 // dq/dt at one cell (or cell pair in the same row i; Kolmogorov forcing varies with i).
 template <unsigned M2, class C>
-FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2)
+FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2,
+                 const Geom<C> &)
 {
   using fg2::fmac;
   using fg2::lit;
@@ -78,7 +89,8 @@ FG2_HD C sound_speed(const C q[NVAR], const fg2::Para<C> &p)
 
 // CFL signal rate of a cell on the Cartesian grid: (|u1| + c_s) / Delta1 + (|u2| + c_s) / Delta2.
 template <class C>
-FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2)
+FG2_HD C signal_rate(const C q[NVAR], const fg2::Para<C> &p, C inv1, C inv2, int i, int j, C delta1, C delta2,
+                     const Geom<C> &)
 {
   (void)i; (void)j; (void)delta1; (void)delta2;
   const C cs = sound_speed<C>(q, p);

@@ -496,13 +496,13 @@ __device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, 
 }
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
-// vr is v of the cell (read stages).  u' and v go straight to HBM; edge cells also write
-// their ghost images.
+// vr is v of the cell (read stages), cg the scheme's geometry of the thread's column.  u' and
+// v go straight to HBM; edge cells also write their ghost images.
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
                                          const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
-                                         typename Store<S>::C &rate)
+                                         typename Store<S>::C &rate, const scheme::Geom<typename Store<S>::C> &cg)
 {
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
@@ -518,7 +518,7 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
 
   T r[NV];
   const T dl1 = SC ? gr.delta1 : a.ks.delta1, dl2 = SC ? gr.delta2 : a.ks.delta2;
-  scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2);
+  scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2, cg);
   if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
   P vn[NP], qp[NP];
 #pragma unroll
@@ -570,7 +570,7 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
       }
       else rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
     }
-    if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2, i, j, dl1, dl2));
+    if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2, i, j, dl1, dl2, cg));
   }
 }
 
@@ -764,6 +764,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
   int n = 0;  // chunks consumed
   int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
   bool whole = false, rim = true;  // the tile lies inside the grid / within HALF cells of an edge
+  scheme::Geom<T> cg{};            // the scheme's geometry of this thread's column (per tile)
   // the stencil's source: the landed box, or (16-bit storage) its decoded copy
   float *dec = reinterpret_cast<float *>(smem + G::DEC_OFF);
 
@@ -795,6 +796,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
       prow0 = i0 - 4 + GT;
       const int th = a.nb * CH;
       whole = i0 + th <= gr.L.n1 && j0 + SW <= gr.L.n2;
+      cg = scheme::column_geom<T>(j0 + tx, SC ? gr.delta2 : a.ks.delta2);
       rim = i0 < HALF || i0 + th > gr.L.n1 - HALF || j0 < HALF || j0 + SW > gr.L.n2 - HALF;
     } else {
       prow0 = i0 + CH * b + 3 + GT;
@@ -824,7 +826,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
     P vrow[NP];                                                                                   \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
     lead_row<T, M2, R, BW * NV>(base, a, st);                                                     \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, whole, rim, nan, rate); \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, whole, rim, nan, rate, cg); \
   }
       FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
