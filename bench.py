@@ -410,7 +410,9 @@ def run_disk_leg(steps, warmup, device):
 def run_precision_leg(n, steps, device):
     """Kelvin-Helmholtz at n x n, the same fixed step sequence in FP64, FP32 and the 16-bit
     deviation storages; per-field L2 (RMS) and Linf errors against the FP64 run, and the
-    relative L2 error of the density rho = exp(lnd)."""
+    relative L2 error of the density rho = exp(lnd).  Also FP32 steps from the initial state
+    rounded once through FP16 deviation storage (`f32_from_f16_start`): the error that a single
+    16-bit rounding of the state leaves, whatever the update does afterwards."""
     import fg2_b200
     state = fg2_b200.setup_evaluate(SETUP, n, n, SCHEME, seed=SEED)[0]
     with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f64") as s:
@@ -425,10 +427,14 @@ def run_precision_leg(n, steps, device):
     rho_ref = np.exp(ref[..., 0])
     rho_norm = np.sqrt((rho_ref ** 2).sum())
     result = {"grid": [n, n], "steps": steps, "dt": dt, "fields": ["lnd", "u1", "u2", "lne"]}
-    for storage in ("f32", "f16", "bf16"):
-        with fg2_b200.Sim(n, n, scheme=SCHEME, storage=storage) as s:
+    with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f16") as s:
+        s.config()
+        s.upload(state32)
+        rounded_start = s.download()  # bg + s h: the state as FP16 deviation storage holds it
+    for storage in ("f32", "f16", "bf16", "f32_from_f16_start"):
+        with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f32" if storage == "f32_from_f16_start" else storage) as s:
             s.config()
-            s.upload(state32)
+            s.upload(rounded_start if storage == "f32_from_f16_start" else state32)
             s.advance(steps, dt)
             status = s.sync()
             out = s.download()
@@ -438,7 +444,7 @@ def run_precision_leg(n, steps, device):
         rho_l2 = float(np.sqrt(((np.exp(out[..., 0].astype(np.float64)) - rho_ref) ** 2).sum()) / rho_norm)
         result[storage] = {"status": status, "l2_rms": rms.tolist(), "linf": linf.tolist(), "rho_rel_l2": rho_l2}
         del out, err
-    for storage in ("f16", "bf16"):
+    for storage in ("f16", "bf16", "f32_from_f16_start"):
         result[storage]["rho_rel_l2_vs_f32"] = result[storage]["rho_rel_l2"] / max(result["f32"]["rho_rel_l2"], 1e-300)
     return result
 
@@ -544,6 +550,10 @@ def run_fused(args):
         torch.cuda.set_device(0)
         tiling = tuple(int(x) for x in args.batch_tiling.split(",")) if args.batch_tiling else None
         print(json.dumps(run_batch_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling, False)), flush=True)
+        return
+    if args.only_precision:  # the 8192^2 precision leg alone
+        torch.cuda.set_device(0)
+        print(json.dumps(run_precision_leg(8192, 500, torch.device("cuda", 0))), flush=True)
         return
     if args.only_disk:  # the disk-scheme leg alone (profiling)
         torch.cuda.set_device(0)
@@ -676,6 +686,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the 16-bit storage and precision legs")
     ap.add_argument("--no-disk", action="store_true", help="skip the disk-scheme leg")
     ap.add_argument("--only-disk", action="store_true", help="run the disk-scheme leg alone and print it")
+    ap.add_argument("--only-precision", action="store_true", help="run the 8192^2 precision leg alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
