@@ -597,16 +597,19 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 }
 
 // Issues the next chunk of the CTA's sequence into its slot (free by the caller's check).
+// `claim` (a register of the issuing thread) holds the queue position of the CTA's next tile:
+// it is drawn when the last chunk of the current tile is issued, one chunk before it is
+// needed, so the atomic's round trip is off the chunk's critical path.
 template <class S, bool READ_V, int W>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
-                                            bool reverse, unsigned extra_bytes, int *queue)
+                                            bool reverse, unsigned extra_bytes, int *queue, int &claim)
 {
   using G = Geo<S, READ_V, W>;
   if (ps->done) return;
   const int n = ps->next_n, s = n % G::NSLOT;
   if (ps->c == 0) {
-    int t = atomicAdd(&queue[0], 1);
+    int t = claim;
     if (t >= ntiles) t = -1;
     else if (reverse) t = ntiles - 1 - t;
     ps->tile = t;
@@ -635,6 +638,7 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     if (with_v)
       tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
                   i0 + CH * (c - 1) + GT);
+    if (c == nb) claim = atomicAdd(&queue[0], 1);  // the next tile's position, used one chunk later
     ps->c = c == nb ? 0 : c + 1;
   }
   ps->next_n = n + 1;
@@ -743,6 +747,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
   int *grid_of = tile_of + NS;
   Producer *ps = reinterpret_cast<Producer *>(grid_of + NS);
 
+  int claim = 0;  // issuing thread: queue position of the CTA's next tile
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
@@ -751,7 +756,8 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
     ps->g = 0;
     ps->c = 0;
     ps->done = 0;
-    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);
+    claim = atomicAdd(&queue[0], 1);
+    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue, claim);
   }
   __syncthreads();
 
@@ -833,7 +839,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
     }
     __syncthreads();  // everyone is done with slot s
     if (threadIdx.x == 0)
-      issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue);  // refill slot s
+      issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue, claim);  // refill slot s
     ++n;
     b = b == a.nb - 1 ? -1 : b + 1;
   }
