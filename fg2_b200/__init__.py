@@ -43,7 +43,7 @@ def _bind(lib):
         "fg2_setup_evaluate": (I, [S, I, I, D, D, P, U64, P]),
         "fg2_sim_create": (P, [I, I, I, P]), "fg2_sim_destroy": (None, [P]),
         "fg2_sim_device_bytes": (SZ, [P]), "fg2_sim_storage": (I, [P]),
-        "fg2_sim_set_box": (I, [P, D, D]), "fg2_sim_set_courant": (I, [P, D]),
+        "fg2_sim_set_box": (I, [P, D, D]), "fg2_sim_set_courant": (I, [P, D]), "fg2_sim_set_tiling": (I, [P, I]),
         "fg2_sim_set_bcond": (I, [P, I, I]), "fg2_sim_para": (S, [P, S]),
         "fg2_sim_get_para": (I, [P, S, ctypes.POINTER(D)]), "fg2_sim_config": (I, [P]),
         "fg2_sim_init": (I, [P, S, U64]), "fg2_sim_upload": (I, [P, P]), "fg2_sim_download": (I, [P, P]),
@@ -174,6 +174,10 @@ class Sim:
 
     def set_courant(self, c):
         self._check(self.lib.fg2_sim_set_courant(self.h, c), "set_courant")
+
+    def set_tiling(self, nb):
+        """Tile height of the fused kernel in blocks of 7 rows (0: the default)."""
+        self._check(self.lib.fg2_sim_set_tiling(self.h, int(nb)), "set_tiling")
 
     def set_bcond(self, p1, p2):
         self._check(self.lib.fg2_sim_set_bcond(self.h, int(p1), int(p2)), "set_bcond")

@@ -70,7 +70,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
                         int p2, double delta1, double delta2, const double *dt, Status *status, int tile0,
                         const DevCode *dev = nullptr, int strip = 0);
 // Tile height of the substage kernel in blocks of 7 output rows, unless a launch sets nb.
-constexpr int TILE_BLOCKS_DEFAULT = 5;
+constexpr int TILE_BLOCKS_DEFAULT = 4;
 // Strip width of single-grid launches; batch launches may also use 64 (strip_width(64)).
 constexpr int STRIP_DEFAULT = 128;
 int strip_width(int strip);

@@ -97,6 +97,7 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.status = s->status;
   a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
   a.wait_test_bytes = s->wait_test_bytes;
+  a.nb = s->nb;
   return a;
 }
 
@@ -123,7 +124,7 @@ int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridD
   StageArgs b = a;
   b.reverse = s->order;
   s->order ^= 1;
-  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L), b, s->queue, s->stream));
+  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L, s->nb), b, s->queue, s->stream));
   return FG2_OK;
 }
 
@@ -485,6 +486,14 @@ int fg2_sim_set_box(fg2_sim *s, double l1, double l2)
   s->l2 = round_para(s, l2);
   s->configured = false;
   drop_graph(s);
+  return FG2_OK;
+}
+
+int fg2_sim_set_tiling(fg2_sim *s, int nb)
+{
+  if (!s || nb < 0 || nb > 64) return fail(FG2_ERR_ARG, "bad tile height %d", nb);
+  if (nb != s->nb) drop_graph(s);
+  s->nb = nb;
   return FG2_OK;
 }
 

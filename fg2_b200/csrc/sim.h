@@ -33,6 +33,7 @@ struct fg2_sim {
   bool desc_valid = false;
   unsigned version = 0;       // bumped whenever settings that descriptors depend on change
   int order = 0;              // tile order of the next substage launch (alternates)
+  int nb = 0;                 // tile height in blocks of 7 rows (0: the default)
   unsigned wait_test_bytes = 0;  // timeout-path tests (fg2_sim_test_stall_waits)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;

@@ -4,7 +4,7 @@
 // Work decomposition.  A launch advances a list of grids (one simulation, or a batch of
 // independent simulations of any sizes).  A tile is a strip of W interior columns (128, or
 // 64 in batch launches) by 7 nb rows of one grid (nb blocks of 7 output rows, a launch
-// parameter, 5 by default); the launch's tiles are numbered grid by grid, strip fastest, and
+// parameter, 4 by default); the launch's tiles are numbered grid by grid, strip fastest, and
 // a persistent grid of CTAs drains them from a queue (an atomic counter that the last CTA to
 // finish resets, so a launch needs no host-side reset and replays from a CUDA graph).  A CTA
 // has W / 32 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in

@@ -77,6 +77,10 @@ int fg2_sim_storage(const fg2_sim *s);
 int fg2_sim_set_box(fg2_sim *s, double l1, double l2);
 int fg2_sim_set_courant(fg2_sim *s, double c);
 int fg2_sim_set_bcond(fg2_sim *s, int p1, int p2);
+/* Tile height of the fused kernel in blocks of 7 rows (0: the default, 4).  No counterpart in
+ * the reference (its block shape came from setup()'s heuristic, src/setup.cpp:39-58); results
+ * are bitwise the same for every height. */
+int fg2_sim_set_tiling(fg2_sim *s, int nb);
 /* para() (src/para.cpp:25-40): "key=val" (leading dashes skipped); returns "key = val" in a
  * buffer owned by the handle, or NULL for an unknown key. */
 const char *fg2_sim_para(fg2_sim *s, const char *keyval);
