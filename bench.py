@@ -173,6 +173,50 @@ def calibrated_sample(state, dt, budget_s, min_steps=1):
     return max(16, min(N1, rows)), steps
 
 
+def run_small_leg(device):
+    """The small plain configuration in full on both sides: hydro 256^2 periodic, rho = 1,
+    p = 1/gamma, Gaussian velocity noise (sigma 0.01, seed 1), the reference's dt, 100 steps;
+    on the GPU (steps replayed from the two-step graph, events on the simulation's stream) and
+    through the reference's CPU arithmetic on all host cores, from the same state."""
+    import torch
+    import fg2_b200
+    from oracle.oracle import Oracle, available, reference_delta
+    n, nsteps = 256, 100
+    with fg2_b200.Sim(n, n) as s:
+        s.config()
+        s.init("noise", seed=1)
+        x0 = s.download()
+        dt = s.getdt()
+        stream = torch.cuda.ExternalStream(s.stream, device=device)
+        s.set_time(0.0)
+        s.advance(10, dt, graph=True)
+        s.upload(x0)
+        s.set_time(0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.advance(nsteps, dt, graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        gpu_ms = e0.elapsed_time(e1)
+        status = s.sync()
+    kind = "reference" if available(SCHEME, "f32", "reference") else "port"
+    o = Oracle(SCHEME, "f32", kind)
+    cores = o.threads(os.cpu_count() or 1)
+    o.set_delta(*reference_delta(n, n, 1.0, 1.0))
+    u = o.padded(x0)
+    v = o.empty(n, n)
+    t0 = time.perf_counter()
+    o.run(u, v, 0.0, dt, nsteps)
+    cpu_s = time.perf_counter() - t0
+    cells = n * n * nsteps
+    return {"workload": "hydro 256x256 periodic, noise sigma 0.01 seed 1, reference dt, 100 steps (in full)",
+            "gpu": {"value": cells / (gpu_ms / 1e3) / 1e9, "unit": "Gcell-steps/s", "ms_per_step": gpu_ms / nsteps,
+                    "status": status, "note": "launch-bound: 64 Kcells per step, all in L2"},
+            "cpu": {"value": cells / cpu_s / 1e9, "unit": "Gcell-steps/s", "seconds": cpu_s, "cores": cores,
+                    "kind": kind}}
+
+
 def initial_state():
     import fg2_b200
     q, _ = fg2_b200.setup_evaluate(SETUP, N1, N2, SCHEME, seed=SEED)
@@ -551,6 +595,10 @@ def run_fused(args):
         tiling = tuple(int(x) for x in args.batch_tiling.split(",")) if args.batch_tiling else None
         print(json.dumps(run_batch_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling, False)), flush=True)
         return
+    if args.only_combined:  # the combined (64-sim FP16 batch) leg alone
+        torch.cuda.set_device(0)
+        print(json.dumps(run_combined_leg(torch.device("cuda", 0))), flush=True)
+        return
     if args.only_precision:  # the 8192^2 precision leg alone
         torch.cuda.set_device(0)
         print(json.dumps(run_precision_leg(8192, 500, torch.device("cuda", 0))), flush=True)
@@ -634,6 +682,10 @@ def run_fused(args):
     if rank == 0 and world == 1 and not args.no_disk and args.storage == "f32":
         disk = run_disk_leg(200, args.warmup, device)
 
+    small = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.storage == "f32":
+        small = run_small_leg(device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
@@ -665,6 +717,7 @@ def run_fused(args):
             "precision": precision,
             "combined": combined,
             "disk": disk,
+            "small": small,
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }
@@ -687,6 +740,7 @@ def main():
     ap.add_argument("--no-disk", action="store_true", help="skip the disk-scheme leg")
     ap.add_argument("--only-disk", action="store_true", help="run the disk-scheme leg alone and print it")
     ap.add_argument("--only-precision", action="store_true", help="run the 8192^2 precision leg alone and print it")
+    ap.add_argument("--only-combined", action="store_true", help="run the combined 64-sim leg alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")

@@ -82,6 +82,25 @@ void compute_deltas(fg2_sim *s)
 // parameters are parsed into R like the reference's atof -> R (src/para.cpp:34)
 double round_para(const fg2_sim *s, double x) { return s->storage == ST_F64 ? x : (double)(float)x; }
 
+// Tile height of the single-grid launches: the caller's, or the default (4 blocks of 7 rows)
+// lowered for grids too small to give every resident CTA a tile (about 3 per SM), down to one
+// block: a 512^2 grid then has 4 x 74 tiles instead of 4 x 19.  Results do not depend on it.
+int tile_height(const fg2_sim *s)
+{
+  if (s->nb > 0) return s->nb;
+  static int sms = 0;  // SMs of the first device seen (the same on every GPU of a node)
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms < 1)
+      sms = 148;
+  }
+  const int want = 3 * sms;
+  int nb = TILE_BLOCKS_DEFAULT;
+  while (nb > 1 && substage_tiles(s->L, nb) < want) --nb;
+  return nb;
+}
+
 StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
 {
   StageArgs a;
@@ -97,7 +116,7 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.status = s->status;
   a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
   a.wait_test_bytes = s->wait_test_bytes;
-  a.nb = s->nb;
+  a.nb = tile_height(s);
   return a;
 }
 
@@ -124,7 +143,7 @@ int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridD
   StageArgs b = a;
   b.reverse = s->order;
   s->order ^= 1;
-  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L, s->nb), b, s->queue, s->stream));
+  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L, b.nb), b, s->queue, s->stream));
   return FG2_OK;
 }
 
