@@ -489,7 +489,7 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   // strip width 128 or 64 columns (4 or 2 warps per CTA); tile height nb blocks of 7 rows;
   // CTAs per SM: 0 = as many as fit (the occupancy limit), or capped at 4, 8 or 12 warps
   for (int strip : {128, 64})
-    for (int nb : {2, 3, 4, 5, 6, 8})
+    for (int nb : {1, 2, 3, 4, 5, 6, 8})
       for (int warps : {0, 4, 8, 12})
         cands.push_back({strip, nb, warps * 32 / strip, std::numeric_limits<double>::infinity()});
   const int keep_nb = b->nb, keep_ctas = b->max_ctas, keep_strip = b->strip;
