@@ -173,6 +173,43 @@ def calibrated_sample(state, dt, budget_s, min_steps=1):
     return max(16, min(N1, rows)), steps
 
 
+# The reference's own benchmark (bench/bench.txt:3-73): hydro-isot FP32 on a Tesla M2090, ms
+# per step at each resolution, the best of its four block shapes.
+REFERENCE_SWEEP_MS = {1024: 5.468, 1280: 12.136, 1536: 14.992, 1792: 18.016, 2048: 21.188, 2560: 47.83,
+                      3072: 59.318, 3584: 71.384, 4096: 84.107, 5120: 151.282, 6144: 189.339, 7168: 285.987,
+                      8192: 337.53, 10240: 526.947, 12288: 758.47, 14336: 1036.88}
+
+
+def run_sweep_leg(device, steps=50, warmup=5):
+    """The reference's benchmark sweep re-run here: hydro-isot FP32, periodic 2 pi box, Gaussian
+    velocity noise (sigma 0.01, seed 7), the reference's dt, at each of its resolutions
+    1024^2 .. 14336^2; steps replayed from the two-step graph, timed with events on the
+    simulation's stream.  Beside each, the reference's published ms per step (Tesla M2090)."""
+    import torch
+    import fg2_b200
+    rows = []
+    for n, ref_ms in REFERENCE_SWEEP_MS.items():
+        with fg2_b200.Sim(n, n, scheme="hydro-isot") as s:
+            s.config()
+            s.init("noise", seed=7)
+            dt = s.getdt()
+            stream = torch.cuda.ExternalStream(s.stream, device=device)
+            s.set_time(0.0)
+            s.advance(warmup, dt, graph=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.advance(steps, dt, graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            status = s.sync()
+        rows.append({"n": n, "ms_per_step": ms, "gcell_steps_per_s": n * n / (ms / 1e3) / 1e9, "status": status,
+                     "reference_m2090_ms_per_step": ref_ms, "speedup_vs_reference": ref_ms / ms})
+    return {"workload": "hydro-isot FP32 periodic, noise sigma 0.01 seed 7, reference dt, "
+                        f"{steps} steps per size (the reference's bench/bench.txt sweep)", "rows": rows}
+
+
 def run_small_leg(device):
     """The small plain configuration in full on both sides: hydro 256^2 periodic, rho = 1,
     p = 1/gamma, Gaussian velocity noise (sigma 0.01, seed 1), the reference's dt, 100 steps;
@@ -595,6 +632,10 @@ def run_fused(args):
         tiling = tuple(int(x) for x in args.batch_tiling.split(",")) if args.batch_tiling else None
         print(json.dumps(run_batch_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling, False)), flush=True)
         return
+    if args.only_sweep:  # the reference's benchmark sweep alone
+        torch.cuda.set_device(0)
+        print(json.dumps(run_sweep_leg(torch.device("cuda", 0))), flush=True)
+        return
     if args.only_combined:  # the combined (64-sim FP16 batch) leg alone
         torch.cuda.set_device(0)
         print(json.dumps(run_combined_leg(torch.device("cuda", 0))), flush=True)
@@ -686,6 +727,10 @@ def run_fused(args):
     if rank == 0 and world == 1 and not args.no_cpu and args.storage == "f32":
         small = run_small_leg(device)
 
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_sweep and args.storage == "f32":
+        sweep = run_sweep_leg(device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
@@ -718,6 +763,7 @@ def run_fused(args):
             "combined": combined,
             "disk": disk,
             "small": small,
+            "sweep": sweep,
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }
@@ -741,6 +787,8 @@ def main():
     ap.add_argument("--only-disk", action="store_true", help="run the disk-scheme leg alone and print it")
     ap.add_argument("--only-precision", action="store_true", help="run the 8192^2 precision leg alone and print it")
     ap.add_argument("--only-combined", action="store_true", help="run the combined 64-sim leg alone and print it")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the reference's benchmark sweep")
+    ap.add_argument("--only-sweep", action="store_true", help="run the reference's benchmark sweep alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
