@@ -162,15 +162,21 @@ def test_device_resident_cfl_steps_track_host_loop(cuda):
 
 def test_batch_members_match_single_grids(cuda):
     sizes = [(40, 48), (64, 32), (24, 60), (130, 67)]
-    with fg2_b200.Batch(sizes, scheme="disk") as b:
-        b.config()
-        states = [smooth(n1, n2, seed=10 + k) for k, (n1, n2) in enumerate(sizes)]
-        for m, x in zip(b.members, states):
-            m.upload(x)
-        b.set_time(0.0)
-        b.advance(10, DT, graph=True)
-        assert b.sync() == 0
-        got = [m.download() for m in b.members]
+    states = [smooth(n1, n2, seed=10 + k) for k, (n1, n2) in enumerate(sizes)]
+    runs = []
+    for strip in (128, 64):  # both strip widths, bitwise alike
+        with fg2_b200.Batch(sizes, scheme="disk") as b:
+            b.config()
+            b.set_strip(strip)
+            for m, x in zip(b.members, states):
+                m.upload(x)
+            b.set_time(0.0)
+            b.advance(10, DT, graph=True)
+            assert b.sync() == 0
+            runs.append([m.download() for m in b.members])
+    got = runs[0]
+    for a, c in zip(*runs):
+        assert np.array_equal(a, c)
     for (n1, n2), x, out in zip(sizes, states, got):
         with fg2_b200.Sim(n1, n2, scheme="disk") as s:
             s.config()
