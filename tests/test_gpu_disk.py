@@ -186,3 +186,27 @@ def test_batch_members_match_single_grids(cuda):
             alone = s.download()
         assert np.all(rel_l2(out, alone) <= 1e-5), ((n1, n2), rel_l2(out, alone))
         assert np.all(rel_l2(out, port_steps(x, 10, DT)) <= 1e-5)
+
+
+def test_reference_mirror_api(cuda):
+    """The function contract of src/fg2.h:70-84 on the disk library: setup / para / config /
+    init / step give what the handle API gives (box and walls from the scheme's settings)."""
+    lib = fg2_b200.load_library("disk")
+    assert lib.fg2_setup(48, 64) > 0
+    assert lib.fg2_para(b"alpha=0.02") == b"alpha = 0.02"
+    lib.fg2_config()
+    lib.fg2_init(b"smooth")
+    assert lib.fg2_getdt() == reference_dt(48, 64, *disk_box(48, 64))
+    for n in range(3):
+        assert lib.fg2_step(n * DT, DT) == 0
+    g = fg2_b200.Sim.__new__(fg2_b200.Sim)
+    g.lib, g.h, g.n1, g.n2, g.nvar, g.host_dtype = lib, lib.fg2_global(), 48, 64, 6, np.float32
+    ug = g.download()
+    g.h = None  # not owned
+    with fg2_b200.Sim(48, 64, scheme="disk") as s:
+        s.para("alpha=0.02")
+        s.config()
+        s.init("smooth", seed=0)
+        for n in range(3):
+            assert s.step(n * DT, DT) == 0
+        assert np.array_equal(s.download(), ug)
