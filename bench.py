@@ -210,6 +210,27 @@ def run_sweep_leg(device, steps=50, warmup=5):
                         f"{steps} steps per size (the reference's bench/bench.txt sweep)", "rows": rows}
 
 
+def accuracy_vs_f64(scheme, n1, n2, x0, steps, dt, para=()):
+    """Per-field RMS and max errors of `steps` FP32 steps against FP64 steps of the same
+    scheme from the same state, with one fixed dt (the FP64 oracle on the GPU: the same kernel
+    in double, itself pinned to the reference's arithmetic at R = double)."""
+    import fg2_b200
+    outs = {}
+    for storage in ("f64", "f32"):
+        with fg2_b200.Sim(n1, n2, scheme=scheme, storage=storage) as s:
+            for kv in para:
+                s.para(kv)
+            s.config()
+            s.upload(x0.astype(np.float64 if storage == "f64" else np.float32))
+            s.set_time(0.0)
+            s.advance(steps, dt)
+            status = s.sync()
+            outs[storage] = s.download().astype(np.float64)
+    err = (outs["f32"] - outs["f64"]).reshape(-1, x0.shape[-1])
+    return {"steps": steps, "dt": dt, "status": status, "l2_rms": np.sqrt((err ** 2).mean(0)).tolist(),
+            "linf": np.abs(err).max(0).tolist()}
+
+
 def run_small_leg(device):
     """The small plain configuration in full on both sides: hydro 256^2 periodic, rho = 1,
     p = 1/gamma, Gaussian velocity noise (sigma 0.01, seed 1), the reference's dt, 100 steps;
@@ -481,9 +502,13 @@ def run_disk_leg(steps, warmup, device):
         status = sim.sync()
     cells = DISK_N * DISK_N
     value = cells * steps / (ms / 1e3) / 1e9
+    nd = 512  # FP32 against FP64 on a smaller grid of the same setup (FP64 disk kernels are slow)
+    x0, _ = fg2_b200.setup_evaluate("smooth", nd, nd, scheme="disk", seed=3)
+    acc = accuracy_vs_f64("disk", nd, nd, x0, 20, 2.0e-6)
     return {"workload": f"disk {DISK_N}x{DISK_N} smooth torus-like state (seed 3), FP32, fixed dt {DISK_DT:g}, walls",
             "value": value, "unit": "Gcell-steps/s", "steps": steps, "ms_per_step": ms / steps, "status": status,
             "gflops_ref_model": value * DISK_FLOP, "flop_per_cell_step": DISK_FLOP,
+            "accuracy_vs_f64": dict(acc, grid=[nd, nd]),
             "roofline": {"bound": "compute", "bytes_per_cell_step": DISK_B_ALG, "hbm_achieved": value * DISK_B_ALG,
                          "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak}}
 
@@ -709,6 +734,10 @@ def run_fused(args):
     if not args.no_e2e:
         e2e, e2e_status = run_e2e(sim, state, stream, args, dist, device, world, cells)
 
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_accuracy and args.storage == "f32":
+        accuracy = accuracy_vs_f64(SCHEME, N1, N2, state, 100, CPU_DT)
+
     batch = None
     if rank == 0 and world == 1 and not args.no_batch and args.storage == "f32":
         batch = run_batch_leg(200, args.warmup, device)
@@ -756,6 +785,7 @@ def run_fused(args):
                          "bytes_per_cell_step": b_alg, "stage_ms": stage_ms},
             "step_hbm_frac": value / world * b_alg / peak,
             "cpu_baseline": cpu,
+            "accuracy_vs_f64": accuracy,
             "e2e": e2e, "e2e_status": e2e_status,
             "batch": batch,
             "mixed": mixed,
@@ -788,6 +818,7 @@ def main():
     ap.add_argument("--only-precision", action="store_true", help="run the 8192^2 precision leg alone and print it")
     ap.add_argument("--only-combined", action="store_true", help="run the combined 64-sim leg alone and print it")
     ap.add_argument("--no-sweep", action="store_true", help="skip the reference's benchmark sweep")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-against-FP64 error of the headline workload")
     ap.add_argument("--only-sweep", action="store_true", help="run the reference's benchmark sweep alone and print it")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
