@@ -349,6 +349,25 @@ def batch_sizes(count=BATCH_COUNT, seed=BATCH_SEED):
     return [(int(x), int(x)) for x in rng.choice(BATCH_SIDES, size=count)]
 
 
+def batch_accuracy(sizes, x0, steps=20, dt=1.0e-3):
+    """FP32 batch against the same batch in FP64 from the same member states, one fixed dt:
+    RMS and max errors per field over all members."""
+    import fg2_b200
+    outs = {}
+    for storage in ("f64", "f32"):
+        with fg2_b200.Batch(sizes, scheme="hydro-isot", storage=storage) as b:
+            b.config()
+            for m, x in zip(b.members, x0):
+                m.upload(x.astype(np.float64 if storage == "f64" else np.float32))
+            b.set_time(0.0)
+            b.advance(steps, dt, graph=True)
+            status = b.sync()
+            outs[storage] = [m.download().astype(np.float64).reshape(-1, 3) for m in b.members]
+    err = np.concatenate([a - c for a, c in zip(outs["f32"], outs["f64"])])
+    return {"steps": steps, "dt": dt, "status": status, "l2_rms": np.sqrt((err ** 2).mean(0)).tolist(),
+            "linf": np.abs(err).max(0).tolist()}
+
+
 def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
     """512 independent hydro-isot simulations (sides 64..512, box 2 pi, random-phase k^-2
     velocity at rms Mach 0.3): one persistent launch per substage over every member's tiles,
@@ -391,11 +410,12 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
     value = cells * steps / (ms / 1e3) / 1e9
     peak, _ = peaks()
     b.close()
+    accuracy = batch_accuracy(sizes, x0) if one_at_a_time else None
 
     result = {"workload": f"{len(sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
                           "box 2 pi, k^-2 random-phase velocity rms Mach 0.3, FP32, per-member CFL dt",
               "cells": cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
-              "status": status, "tiling": {"strip_columns": strip, "warps_per_cta": strip // 32, "blocks_of_7_rows": nb,
+              "status": status, "accuracy_vs_f64": accuracy, "tiling": {"strip_columns": strip, "warps_per_cta": strip // 32, "blocks_of_7_rows": nb,
                          "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
               "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
                            "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
