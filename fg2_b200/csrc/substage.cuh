@@ -13,7 +13,7 @@
 //
 // Data movement.  u and v stream through a ring of NSLOT shared-memory slots by TMA
 // (cp.async.bulk.tensor.3d, no multicast): chunk 0 of a tile is the 7-row warm-up box
-// u[i0-4 .. i0+3) x [j0-4, j0+132), chunk b+1 the 7 leading rows u[i0+3+7b ..] of output
+// u[i0-4 .. i0+3) x [j0-4, j0+W+4), chunk b+1 the 7 leading rows u[i0+3+7b ..] of output
 // block b together with v of the block's 7 output rows.  A box lands as [row][cell][field],
 // the cells' fields interleaved as in HBM, so a thread reads a whole hydro cell with one
 // 16-byte shared load.  The results u' and v are written by the threads straight from
@@ -28,9 +28,11 @@
 // L-3 then needs no further loads), and feeds the mixed derivative by streaming accumulators:
 // with delta_k(r) = u(r, j+k) - u(r, j-k), D12(r) = sum_k m_k (delta_k(r+k) - delta_k(r-k)),
 // so delta_k(L) is added to row L-k and subtracted from row L+k (src/deriv.h:60-62
-// regrouped).  Fields are handled in pairs ((lnd, u1), (u2, lne)) so the stencil arithmetic of
-// two fields is one packed FP32x2 instruction (add/mul/fma .f32x2 on sm_100).  The output row
-// L-3 then has all its derivatives in registers; the scheme's eqns() gives F, and the
+// regrouped).  Fields are handled in pairs ((lnd, u1), (u2, lne) for hydro; up to three pairs)
+// so the stencil arithmetic of two fields is one packed FP32x2 instruction (add/mul/fma .f32x2
+// on sm_100); the mixed derivative is accumulated for the scheme's D12 fields only.  The output row
+// L-3 then has all its derivatives in registers; the scheme's eqns() gives F (with the cell's
+// indices, the spacings and the scheme's per-column geometry, computed once per tile), and the
 // epilogue applies v <- F + beta v, u' <- u + gamma dt v (src/kick.cu:53, src/drift.cu:29),
 // stores u' with its ghost images and v, flags NaNs and, on the last stage, folds the CFL rate
 // into a max.  Register slots are indexed by row mod 7 and the row loop is unrolled by 7, so
