@@ -161,3 +161,57 @@ def test_isot_setups_use_the_2pi_box():
     assert known
     x = 2 * np.pi * (np.arange(8) + 0.5) / 8
     np.testing.assert_allclose(q[:, 0, 2], 0.1 / (0.01 * 4) * np.cos(2 * x), atol=1e-7)
+
+
+def _centres(n1, n2, l1=1.0, l2=1.0):
+    x = l1 * (np.arange(n1) + 0.5) / n1 - 0.5 * l1
+    y = l2 * (np.arange(n2) + 0.5) / n2 - 0.5 * l2
+    return np.meshgrid(x, y, indexing="ij")
+
+
+def _fermi_dirac(x, d):
+    return 1.0 / (np.exp(x / d) + 1.0)
+
+
+@pytest.mark.parametrize("name", ["blast", "bow", "implos", "Sod"])
+def test_reference_hydro_setups(name):
+    """The reference's named initial conditions (src/hydro/init.h:26-94) at cell centres of the
+    unit box, restated here in numpy: (ln rho, u1, u2, ln e)."""
+    n1, n2, g = 40, 56, 5.0 / 3.0
+    q, known = fg2_b200.setup_evaluate(name, n1, n2, "hydro")
+    assert known
+    X, Y = _centres(n1, n2)
+    zero = np.zeros_like(X)
+    if name == "blast":
+        e = np.where(X * X + Y * Y < 0.01, 1.0, 0.01) / (g - 1.0)
+        ref = [zero, zero, zero, np.log(e)]
+    elif name == "bow":
+        d = 9.9 * _fermi_dirac(np.sqrt(X * X + Y * Y) - 0.01, 0.001) + 0.1
+        ref = [np.log(d), (10.0 / d - 1.0) / 99.0, zero, np.log(0.01 / d / (g - 1.0))]
+    elif name == "implos":
+        f = _fermi_dirac(0.15 - np.abs(X) - np.abs(Y), 0.001)
+        d, p = 0.125 + 0.875 * f, 0.14 + 0.86 * f
+        ref = [np.log(d), zero, zero, np.log(p / d / (g - 1.0))]
+    else:
+        left = np.fmod(X - 2 * Y + 1.5, 1.0) < 0.5
+        d, p = np.where(left, 1.0, 0.125), np.where(left, 1.0, 0.1)
+        ref = [np.log(d), zero, zero, np.log(p / d / (g - 1.0))]
+    np.testing.assert_allclose(q, np.stack(ref, axis=-1), rtol=1e-12, atol=1e-14)
+
+
+def test_reference_kh_setup_is_a_seeded_step_profile():
+    """src/hydro/init.h:60-76: rho 2 and u1 = 0.5 within |y| < 1/4, rho 1 and u1 = -0.5 outside,
+    each u1 plus uniform noise in [-0.005, 0.005) (rand() replaced by the seeded generator),
+    p = 2.5."""
+    n1, n2, g = 32, 48, 5.0 / 3.0
+    q, known = fg2_b200.setup_evaluate("KH", n1, n2, "hydro", seed=9)
+    assert known
+    _, Y = _centres(n1, n2)
+    inner = np.abs(Y) < 0.25
+    np.testing.assert_allclose(np.exp(q[..., 0]), np.where(inner, 2.0, 1.0), rtol=1e-14)
+    noise = q[..., 1] - np.where(inner, 0.5, -0.5)
+    assert np.all(np.abs(noise) <= 0.005 + 1e-15) and noise.std() > 0.002
+    np.testing.assert_allclose(np.exp(q[..., 0]) * (g - 1) * np.exp(q[..., 3]), 2.5, rtol=1e-13)
+    assert np.all(q[..., 2] == 0)
+    q2, _ = fg2_b200.setup_evaluate("KH", n1, n2, "hydro", seed=9)
+    assert np.array_equal(q, q2)
