@@ -368,20 +368,24 @@ def batch_accuracy(sizes, x0, steps=20, dt=1.0e-3):
             "linf": np.abs(err).max(0).tolist()}
 
 
-def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
+def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0, world=1, dist=None):
     """512 independent hydro-isot simulations (sides 64..512, box 2 pi, random-phase k^-2
     velocity at rms Mach 0.3): one persistent launch per substage over every member's tiles,
     two-step CUDA graph, per-member device-resident CFL steps, autotuned tiling.  Beside it,
     the same simulations advanced one after another through the single-grid path on one
-    stream (one two-step graph per simulation)."""
+    stream (one two-step graph per simulation).  With world > 1 every rank steps its share of
+    the 512 members (fg2_b200.shard_members, by cell count; member k keeps its seed), with no
+    exchange; the rate is all members' cell-steps over the slowest rank's time."""
     import torch
     import fg2_b200
-    sizes = batch_sizes()
+    all_sizes = batch_sizes()
+    mine = fg2_b200.shard_members(all_sizes, world)[rank]
+    sizes = [all_sizes[k] for k in mine]
     two_pi = 2 * np.pi
     b = fg2_b200.Batch(sizes, scheme="hydro-isot")
     b.set_box(two_pi, two_pi)
     b.config()
-    for k, m in enumerate(b.members):
+    for m, k in zip(b.members, mine):
         m.init("turb", seed=BATCH_SEED * 100000 + k)
     x0 = [m.download() for m in b.members]
     if tiling:
@@ -401,26 +405,32 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True):
         raise RuntimeError("batch warm-up produced a bad status")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    barrier(dist, device)
+    torch.cuda.synchronize()
     e0.record(stream)
     b.advance(steps, 0.0, graph=True)
     e1.record(stream)
     e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    status = b.sync()
-    value = cells * steps / (ms / 1e3) / 1e9
+    ms = reduce_max(e0.elapsed_time(e1), dist, device)
+    status = int(reduce_max(b.sync(), dist, device))
+    total_cells = sum(a * c for a, c in all_sizes)
+    value = total_cells * steps / (ms / 1e3) / 1e9
     peak, _ = peaks()
     b.close()
     accuracy = batch_accuracy(sizes, x0) if one_at_a_time else None
 
-    result = {"workload": f"{len(sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
+    result = {"workload": f"{len(all_sizes)} hydro-isot sims, sides {list(BATCH_SIDES)} drawn with seed {BATCH_SEED}, "
                           "box 2 pi, k^-2 random-phase velocity rms Mach 0.3, FP32, per-member CFL dt",
-              "cells": cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
+              "cells": total_cells, "steps": steps, "value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps,
               "status": status, "accuracy_vs_f64": accuracy, "tiling": {"strip_columns": strip, "warps_per_cta": strip // 32, "blocks_of_7_rows": nb,
                          "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
               "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
                            "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
                            "frac": value * B_ALG_ISOT / peak},
               "gpu_launches_per_step": 4}
+    if world > 1:
+        result.update(n_gpus=world, scaling="strong", sharding="members by cell count, no exchange",
+                      rank0_members=len(sizes), rank0_cells=cells, ms_per_step_max_over_ranks=ms / steps)
     if not one_at_a_time:
         return result
 
@@ -759,8 +769,10 @@ def run_fused(args):
         accuracy = accuracy_vs_f64(SCHEME, N1, N2, state, 100, CPU_DT)
 
     batch = None
-    if rank == 0 and world == 1 and not args.no_batch and args.storage == "f32":
-        batch = run_batch_leg(200, args.warmup, device)
+    if not args.no_batch and args.storage == "f32":
+        # N > 1: every rank steps its share of the members (the same collective steps on all)
+        batch = run_batch_leg(200, args.warmup, device, one_at_a_time=world == 1, rank=rank, world=world,
+                              dist=dist)
 
     mixed, precision, combined = None, None, None
     if rank == 0 and world == 1 and not args.no_mixed and args.storage == "f32":

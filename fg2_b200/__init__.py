@@ -408,3 +408,21 @@ class Batch:
         ms = ctypes.c_double()
         self._check(self.lib.fg2_batch_autotune(self.h, int(reps), ctypes.byref(ms)), "autotune")
         return ms.value
+
+
+def shard_members(sizes, world):
+    """Split a batch's members over `world` ranks by cell count: members in descending cell
+    count (ties by index) each go to the rank holding the fewest cells so far (lowest rank on a
+    tie).  Returns, per rank, the sorted member indices it owns.  Members are independent, so
+    the ranks step their shards with no exchange; the heaviest rank holds at most the mean plus
+    one member.  The reference runs one simulation on one device and has no multi-device path."""
+    world = int(world)
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0] * world
+    shards = [[] for _ in range(world)]
+    for k in sorted(range(len(sizes)), key=lambda k: (-sizes[k][0] * sizes[k][1], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        shards[r].append(k)
+        load[r] += sizes[k][0] * sizes[k][1]
+    return [sorted(s) for s in shards]

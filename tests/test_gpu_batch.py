@@ -210,3 +210,28 @@ def test_nan_in_one_member_is_reported(cuda):
         assert b.sync() == 1
         assert b.members[1].sync() == 1
         assert b.members[0].sync() == 0
+
+
+def test_member_shards_step_like_the_whole_batch(cuda):
+    """A batch split over ranks by fg2_b200.shard_members: each shard, stepped as its own
+    batch with device CFL steps, gives bitwise the member states and times of the whole batch
+    (members share no data; each member's dt is its own)."""
+    sizes = [(64, 64), (96, 128), (192, 64), (128, 128), (64, 96), (256, 192), (96, 96)]
+
+    def run(idx):
+        with fg2_b200.Batch([sizes[k] for k in idx], scheme="hydro-isot") as b:
+            b.set_box(TWO_PI, TWO_PI)
+            b.config()
+            for m, k in zip(b.members, idx):
+                m.init("turb", seed=50 + k)
+            b.set_tiling(4, 0)
+            b.set_time(0.0)
+            assert b.advance(6, 0.0, graph=True) == 0
+            assert b.sync() == 0
+            return {k: (m.download(), m.time()) for m, k in zip(b.members, idx)}
+
+    whole = run(list(range(len(sizes))))
+    for world in (2, 3):
+        for shard in fg2_b200.shard_members(sizes, world):
+            for k, (x, t) in run(shard).items():
+                assert np.array_equal(x, whole[k][0]) and t == whole[k][1], (world, k)
