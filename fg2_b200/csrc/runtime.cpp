@@ -638,10 +638,12 @@ double fg2_sim_getdt(fg2_sim *s)
     const float den = (float)s->n1 / (float)s->l1 + (float)s->n2 / (float)s->l2;
     return (double)(float)s->c / (double)den;
   }
-  if (cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream) != cudaSuccess ||
-      launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status, s->stream,
-                        dev_code(s)) !=
-          cudaSuccess ||
+  // the last step() already took the signal max of the current state in its last stage;
+  // otherwise (after an upload, a user drift, a fixed-dt run) one reduction pass takes it
+  const bool reduce = !s->smax_valid;
+  if ((reduce && (cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream) != cudaSuccess ||
+                  launch_signal_max(s->storage, s->u[s->cur], s->L, s->para, s->delta1, s->delta2, s->status,
+                                    s->stream, dev_code(s)) != cudaSuccess)) ||
       cudaMemcpyAsync(s->status_host, s->status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess) {
     fail(FG2_ERR_ARG, "getdt reduction failed");
@@ -662,7 +664,11 @@ int fg2_sim_step(fg2_sim *s, double t, double dt)
   (void)t;  // passed to the equations by the reference but unused by them (src/kick.cu:98)
   if (!s) return fail(FG2_ERR_ARG, "null handle");
   ensure_config(s);
-  int rc = enqueue_step(s, dt, nullptr, false);
+  // with CFL time steps the last stage also takes the signal max of the new state, which the
+  // next getdt() reads instead of a separate reduction pass
+  const bool cfl = s->dt_mode != FG2_DT_REFERENCE;
+  if (cfl) CK(cudaMemsetAsync(&s->status->smax, 0, sizeof(unsigned long long), s->stream));
+  int rc = enqueue_step(s, dt, nullptr, cfl);
   if (rc) return rc;
   return read_status(s);
 }

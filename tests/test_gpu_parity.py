@@ -213,6 +213,30 @@ def test_cfl_getdt_matches_host_reduction(cuda):
     assert dt == pytest.approx(min(0.5 / rate, dt_diff), rel=1e-12)
 
 
+def test_getdt_after_a_step_reads_the_fused_max(cuda):
+    """With CFL time steps, step() takes the signal max of the new state in its last stage and
+    the next getdt() reads it: the same dt as a reduction pass over that state (the fused rate
+    is evaluated in FP32, the pass in FP64), and the state is bitwise the one a step with the
+    reference's getdt mode gives for the same dt."""
+    n1, n2 = 64, 80
+    with fg2_b200.Sim(n1, n2) as a, fg2_b200.Sim(n1, n2) as b, fg2_b200.Sim(n1, n2) as c:
+        for s in (a, b, c):
+            s.config()
+            s.init("kh", seed=4)
+        a.set_dt_mode("cfl")
+        b.set_dt_mode("cfl")
+        t = 0.0
+        for _ in range(3):
+            dt = a.getdt()
+            assert a.step(t, dt) == 0 and c.step(t, dt) == 0
+            t += dt
+        fused = a.getdt()
+        assert a.getdt() == fused  # no state change, no new max
+        b.upload(a.download())
+        assert fused == pytest.approx(b.getdt(), rel=1e-6)
+        assert np.array_equal(a.download(), c.download())
+
+
 def test_device_resident_dt_tracks_host_loop(cuda):
     """advance(dt <= 0): getdt fused into the last stage, dt and t kept on the device."""
     n1, n2, nsteps = 64, 64, 8
