@@ -312,6 +312,7 @@ int transfer(fg2_sim *s, void *dev_array, void *host, bool to_device)
 void drop_graph(fg2_sim *s)
 {
   s->desc_valid = false;
+  s->smax_valid = false;  // the signal max depends on the parameters, box and spacings too
   ++s->version;
   for (int b = 0; b < 2; ++b) {
     if (s->graph[b]) cudaGraphExecDestroy(s->graph[b]);

@@ -235,6 +235,13 @@ def test_getdt_after_a_step_reads_the_fused_max(cuda):
         b.upload(a.download())
         assert fused == pytest.approx(b.getdt(), rel=1e-6)
         assert np.array_equal(a.download(), c.download())
+        # a parameter or box change makes the kept max stale: getdt() takes a new one
+        assert a.step(t, a.getdt()) == 0
+        for s in (a, b):
+            assert s.para("gamma=1.4") is not None
+            s.set_box(1.0, 0.8)
+        b.upload(a.download())
+        assert a.getdt() == b.getdt()
 
 
 def test_device_resident_dt_tracks_host_loop(cuda):
