@@ -36,6 +36,7 @@ B_STAGE = [3 * NVAR * ELEM, 4 * NVAR * ELEM, 3 * NVAR * ELEM]
 B_ALG = sum(B_STAGE)  # 160 B per cell-step
 METRIC = "Gcell-steps/s"
 CPU_DT = 1.8e-5  # fixed step of the CPU samples: inside this workload's CFL/diffusive limit (~1.86e-5)
+DATA = "synthetic: seeded tanh Kelvin-Helmholtz shear layer (setup kh, seed 2)"
 WORKLOAD = "hydro 4096x4096 periodic tanh Kelvin-Helmholtz, plain FP32 fused RK3 step, device-resident CFL dt"
 
 
@@ -281,11 +282,22 @@ def initial_state():
     return q.astype(np.float32)
 
 
+def config_of(storage, world):
+    """The workload's `config` object, the same in both arms."""
+    return {"workload": WORKLOAD if storage == "f32" else WORKLOAD.replace("plain FP32", f"{storage} deviation storage"),
+            "storage": storage, "scheme": SCHEME, "grid": [N1, N2], "setup": SETUP, "seed": SEED,
+            "dt": "CFL + diffusive limit, FP64, device-resident", "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (u, u' and v are 268 MB each)"}
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
-    state = initial_state()
+    # the input comes from the numpy restatement of the setup, so this process maps no
+    # library of the product: only the reference's arithmetic compiled for the host
+    from oracle.setups import kh
+    state = kh(N1, N2, seed=SEED).astype(np.float32)
     dt = CPU_DT
     rows, per = calibrated_sample(state, dt, 120.0 / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
@@ -298,8 +310,8 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / (args.steps * per) * 1e3 * (N1 / rows),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "scheme": SCHEME, "grid": [N1, N2]},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
+        "config": config_of(args.storage, world),
         "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
                          "sample": f"each step: {per} RK3 step(s) on a periodic {rows}x{N2} strip of the 4096^2 state"},
         "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -829,11 +841,8 @@ def run_fused(args):
             "metric": METRIC, "value": value, "unit": "Gcell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.storage == "f32" else f"{args.storage} storage, f32 math",
-            "data": "synthetic: seeded tanh Kelvin-Helmholtz shear layer (setup kh, seed 2)",
-            "config": {"workload": WORKLOAD if args.storage == "f32" else WORKLOAD.replace("plain FP32", f"{args.storage} deviation storage"),
-                       "storage": args.storage, "scheme": SCHEME, "grid": [N1, N2], "setup": SETUP, "seed": SEED,
-                       "dt": "CFL + diffusive limit, FP64, device-resident", "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (u, u' and v are 268 MB each)"},
+            "data": DATA,
+            "config": config_of(args.storage, world),
             "ns_per_cell_step": 1.0 / (value / world),
             "status": status, "sim_time": sim_time,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -65,6 +65,7 @@ def _bind(lib):
         "fg2_kick": (None, [P, P, ctypes.c_float, ctypes.c_float]),
         "fg2_drift": (None, [P, P, ctypes.c_float]), "fg2_bcond": (None, [P, I, I]),
         "fg2_Euler": (None, [P, ctypes.c_float]), "fg2_global": (P, []),
+        "fg2_u": (P, []), "fg2_v": (P, []), "fg2_s": (ctypes.c_longlong, []),
         "fg2_sums_noalloc": (I, [P, I, I, LL, I, P, P]),
         "fg2_sim_solve": (I, [P, D, D, I, I, S, ctypes.POINTER(D)]),
         "fg2_sim_test_stall_waits": (I, [P, I]),

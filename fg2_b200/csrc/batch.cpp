@@ -467,6 +467,8 @@ int fg2_batch_sync(fg2_batch *b)
   for (int k = 0; k < b->count; ++k) {
     err |= b->status_host[k].error;
     nan |= b->status_host[k].nan;
+    // a signal max folded into a stage that gave up or produced a NaN is not the state's
+    if (b->status_host[k].error || b->status_host[k].nan) b->members[k]->smax_valid = false;
   }
   if (err) return fail(FG2_ERR_TIMEOUT, "a bounded in-kernel wait gave up (bits %u)", err);
   if (nan) return fail(FG2_ERR_NAN, "NaN in a batch member");

@@ -15,7 +15,11 @@
 //     streams, two threads, two host processes sharing a context) race; serialise them;
 //   - each call overwrites every partial it reads, so nothing needs clearing between calls;
 //   - the first call on a device resolves the array's device address (cudaGetSymbolAddress)
-//     with that device current; make that first call before any stream capture.
+//     with that device current; make that first call before any stream capture.  The
+//     address is kept per device and CUDA context: after the caller resets the device (a new
+//     primary context) the next call resolves it again;
+//   - `stream` must belong to the current device (checked).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -37,10 +41,30 @@ constexpr int MAX_DEVICES = 64;
 // One partial (rho, rho u1, rho u2, energy) per grid row: 16384 x 4 doubles = 512 KiB.
 __device__ __align__(256) double noalloc_scratch[NOALLOC_MAX_ROWS * 4];
 
-// Host-side cache of the array's device address per device.  In host code the name
-// noalloc_scratch is only a host stand-in, never a device address.
+// Host-side cache of the array's device address per device, with the context it was
+// resolved in.  In host code the name noalloc_scratch is only a host stand-in, never a
+// device address.
 double *g_scratch[MAX_DEVICES] = {};
+CUcontext g_scratch_ctx[MAX_DEVICES] = {};
 std::mutex g_scratch_mu;
+
+// The calling thread's current CUDA context (driver entry point, resolved once).
+CUcontext current_context()
+{
+  using Fn = CUresult (*)(CUcontext *);
+  static Fn get = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get = (Fn)fn;
+  });
+  CUcontext c = nullptr;
+  if (get && get(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
 
 // Block i sums row i: thread t takes columns t, t + 256, ... in order, then a fixed tree.
 template <class T>
@@ -97,13 +121,15 @@ int scratch_address(double **out)
   if (e != cudaSuccess) return set_error((int)e, "cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= MAX_DEVICES) return set_error(FG2_ERR_ARG, "device %d out of range", dev);
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch[dev]) {
+  const CUcontext ctx = current_context();
+  if (!g_scratch[dev] || g_scratch_ctx[dev] != ctx) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, noalloc_scratch);
     if (e != cudaSuccess || !p)
       return set_error(e != cudaSuccess ? (int)e : FG2_ERR_ARG, "cudaGetSymbolAddress of the scratch array failed: %s",
                        cudaGetErrorString(e));
     g_scratch[dev] = (double *)p;
+    g_scratch_ctx[dev] = current_context();  // the runtime call made the primary context current
   }
   *out = g_scratch[dev];
   return FG2_OK;
@@ -126,6 +152,17 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
     return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: pitch %lld too small for %d x %d", pitch, n1, n2);
   if (storage != ST_F32 && storage != ST_F64)
     return set_error(FG2_ERR_UNSUPPORTED, "fg2_sums_noalloc: storage %d not supported", storage);
+  // an error left on this thread by earlier, unrelated work would otherwise be reported
+  // as this call's launch failure
+  (void)cudaGetLastError();
+  cudaStream_t s = (cudaStream_t)stream;
+  int cur = 0, sdev = 0;
+  cudaError_t de = cudaGetDevice(&cur);
+  if (de == cudaSuccess) de = cudaStreamGetDevice(s, &sdev);
+  if (de != cudaSuccess) return set_error((int)de, "fg2_sums_noalloc: %s", cudaGetErrorString(de));
+  if (sdev != cur)
+    return set_error(FG2_ERR_ARG, "fg2_sums_noalloc: the stream belongs to device %d, the current device is %d", sdev,
+                     cur);
   double *scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;
@@ -134,7 +171,6 @@ extern "C" int fg2_sums_noalloc(const void *u, int n1, int n2, long long pitch, 
   L.n2 = n2;
   L.RS = pitch;
   L.CS = scheme::NVAR;
-  cudaStream_t s = (cudaStream_t)stream;
   if (storage == ST_F32) row_sums_kernel<float><<<n1, NA_THREADS, 0, s>>>((const float *)u, L, scratch);
   else row_sums_kernel<double><<<n1, NA_THREADS, 0, s>>>((const double *)u, L, scratch);
   rows_final_kernel<<<1, NA_THREADS, 0, s>>>(scratch, n1, out);

@@ -229,6 +229,8 @@ int read_status(fg2_sim *s)
   CK(cudaMemcpyAsync(s->status_host, s->status, sizeof(Status), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
+  // a signal max folded into a stage that gave up or produced a NaN is not the state's
+  if (s->status_host->error || s->status_host->nan) s->smax_valid = false;
   if (s->status_host->error) return fail(FG2_ERR_TIMEOUT, "a bounded in-kernel wait gave up (bits %u)", s->status_host->error);
   if (s->status_host->nan) return fail(FG2_ERR_NAN, "NaN in the state");
   return FG2_OK;
@@ -1042,13 +1044,26 @@ void fg2_dump(const char *path, double time) { if (g_sim) fg2_sim_dump(g_sim, pa
 double fg2_getdt(void) { return g_sim ? fg2_sim_getdt(g_sim) : 0.0; }
 int fg2_step(double t, double dt) { return g_sim ? fg2_sim_step(g_sim, t, dt) : FG2_ERR_ARG; }
 
-// kick/drift/bcond/Euler take device pointers into arrays of the global layout, as the
-// reference's take interior-origin pointers (src/fg2.h:81-84).
+// The process-wide simulation's arrays as the reference's globals hold them: interior-origin
+// pointers (element (f, i, j) at p[i * s + j * NVAR + f], ghosts at negative i, j) and the row
+// stride s in elements (src/setup.cpp:64-72: global::u = base + HALF (s + NVAR)).  Here the
+// interior starts one padding column further in, so the offset is 3 s + 4 NVAR.
+static long long interior_offset(const fg2_sim *s) { return s->L.at(0, 0, 0); }
+float *fg2_u(void) { return g_sim ? (float *)g_sim->u[g_sim->cur] + interior_offset(g_sim) : nullptr; }
+float *fg2_v(void) { return g_sim ? (float *)g_sim->v + interior_offset(g_sim) : nullptr; }
+long long fg2_s(void) { return g_sim ? g_sim->L.RS : 0; }
+
+// kick/drift/bcond/Euler take interior-origin device pointers into arrays of the global
+// layout, as the reference's do (src/fg2.h:81-84 called with global::u, global::v).
+static float *array_base(const float *p) { return const_cast<float *>(p) - interior_offset(g_sim); }
+
 void fg2_kick(float *v, const float *u, float t, float beta)
 {
   (void)t;
-  if (!g_sim) return;
+  if (!g_sim || !v || !u) return;
   ensure_config(g_sim);
+  v = array_base(v);
+  u = array_base(u);
   // any arrays of the global layout: the descriptor is encoded for these pointers
   GridDesc &d = g_sim->desc_host[2];
   if (make_grid_desc(&d, u, nullptr, v, g_sim->L, g_sim->storage, g_sim->p1, g_sim->p2, g_sim->delta1, g_sim->delta2,
@@ -1066,7 +1081,9 @@ void fg2_kick(float *v, const float *u, float t, float beta)
 
 void fg2_drift(float *u, const float *v, float dt)
 {
-  if (!g_sim) return;
+  if (!g_sim || !u || !v) return;
+  u = array_base(u);
+  v = array_base(v);
   launch_drift(g_sim->storage, u, v, g_sim->L, dt, g_sim->status, g_sim->stream);
   if (u == g_sim->u[g_sim->cur]) { g_sim->ghosts_valid = false; g_sim->smax_valid = false; }
   cudaStreamSynchronize(g_sim->stream);
@@ -1074,15 +1091,18 @@ void fg2_drift(float *u, const float *v, float dt)
 
 void fg2_bcond(float *u, int p1, int p2)
 {
-  if (!g_sim) return;
+  if (!g_sim || !u) return;
+  u = array_base(u);
   launch_bcond(g_sim->storage, u, g_sim->L, p1 ? BC_PERIODIC : BC_WALL, p2 ? BC_PERIODIC : BC_WALL, g_sim->stream);
   cudaStreamSynchronize(g_sim->stream);
 }
 
 void fg2_Euler(float *u, float dt)
 {
-  if (!g_sim) return;
+  if (!g_sim || !u) return;
   ensure_config(g_sim);
+  u = array_base(u);
+  if (u == g_sim->u[g_sim->cur]) { g_sim->ghosts_valid = false; g_sim->smax_valid = false; }
   if (!g_sim->fixed_phases) {
     g_sim->r1 = (float)(6.2831853071795865 * g_sim->forcing.uniform());
     g_sim->r2 = (float)(6.2831853071795865 * g_sim->forcing.uniform());

@@ -2,8 +2,8 @@
  * include/fg2_b200.h -- C ABI of the B200-native fg2 time step.
  *
  * One shared library per scheme, as the reference builds one binary per scheme directory
- * (Makefile:19-22, `make hydro` -> bin/hydro): libfg2_hydro.so and libfg2_hydro-isot.so
- * export the same symbols.  Plain C types only; device pointers are `void *`.
+ * (Makefile:19-22, `make hydro` -> bin/hydro): libfg2_hydro.so, libfg2_hydro-isot.so and
+ * libfg2_disk.so export the same symbols.  Plain C types only; device pointers are `void *`.
  *
  * Two layers:
  *   - the handle API (fg2_sim_*): explicit simulation objects, a caller-chosen CUDA stream,
@@ -213,6 +213,14 @@ double fg2_load(const char *path);
 void fg2_dump(const char *path, double time);
 double fg2_getdt(void);
 int fg2_step(double t, double dt);
+/* The process-wide simulation's arrays as the reference's globals hold them
+ * (src/setup.cpp:64-72, global::u, global::v, global::s): interior-origin device pointers,
+ * element (f, i, j) at p[i * s + j * NVAR + f] with ghosts at negative i and j, and the row
+ * stride s in elements.  The state ping-pongs between two arrays, so fg2_u() changes with
+ * every step.  kick/drift/bcond/Euler take pointers of this form, as the reference's do. */
+float *fg2_u(void);
+float *fg2_v(void);
+long long fg2_s(void);
 void fg2_kick(float *v, const float *u, float t, float beta);
 void fg2_drift(float *u, const float *v, float dt);
 void fg2_bcond(float *u, int p1, int p2);

@@ -204,8 +204,12 @@ def make_case(name, scheme, prec, n1, n2, init, para, steps, p1, p2, rand, seed)
     )
 
 
+# The reference tree these vectors are made from (read-only); FG2_REFERENCE overrides it.
+REFERENCE_TREE = os.environ.get("FG2_REFERENCE", "/root/reference")
+
+
 def main(prefixes=()):
-    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "REF=" + REFERENCE_TREE])
     for seed, case in enumerate(CASES, start=1):
         if prefixes and not any(case[0].startswith(p) for p in prefixes):
             continue

@@ -338,3 +338,52 @@ def test_reference_mirror_api(cuda):
         for n in range(3):
             assert s.step(n * dt, dt) == 0
         assert np.array_equal(s.download(), ug)
+
+
+def test_reference_mirror_api_takes_interior_origin_pointers(cuda):
+    """fg2_u/fg2_v/fg2_s hand out the arrays as the reference's globals hold them
+    (global::u = base + HALF (s + NVAR), src/setup.cpp:64-72), and fg2_bcond / fg2_kick /
+    fg2_drift, called with those pointers the way src/step.cpp:30-35 calls bcond / kick /
+    drift, give what the handle API's bcond / kick / drift give."""
+    import torch
+
+    class DevArray:  # a view of device memory at a raw address (CUDA array interface)
+        def __init__(self, ptr, n):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 3}
+
+    lib = fg2_b200.load_library("hydro")
+    n1, n2 = 40, 72
+    assert lib.fg2_setup(n1, n2) > 0
+    lib.fg2_config()
+    lib.fg2_init(b"noise")
+    s_el = lib.fg2_s()
+    u, v = lib.fg2_u(), lib.fg2_v()
+    g = fg2_b200.Sim.__new__(fg2_b200.Sim)
+    g.lib, g.h, g.n1, g.n2, g.nvar, g.host_dtype = lib, lib.fg2_global(), n1, n2, 4, np.float32
+    pitch, cell = g.layout()
+    assert s_el == pitch and cell == 4
+    x = g.download()
+    # the interior-origin pointer indexes the interior like the reference: u[i s + j NVAR + f],
+    # row -1 and column -1 are ghosts
+    torch.cuda.synchronize()
+    whole = torch.as_tensor(DevArray(u, (n1 - 1) * s_el + n2 * 4), device=cuda).cpu().numpy()
+    for i, j in ((0, 0), (17, 33), (n1 - 1, n2 - 1)):
+        assert np.array_equal(whole[i * s_el + j * 4: i * s_el + j * 4 + 4], x[i, j])
+    # one RK3 substage by hand through the mirror API (src/step.cpp:30-35, i = 0)
+    dt = lib.fg2_getdt()
+    lib.fg2_bcond(u, 1, 1)
+    lib.fg2_kick(v, u, 0.0, 0.0)
+    lib.fg2_drift(u, v, dt / 3.0)
+    torch.cuda.synchronize()
+    ghost = torch.as_tensor(DevArray(u - 4 * (s_el + 4), 4), device=cuda).cpu().numpy()
+    out_mirror = g.download()
+    g.h = None  # not owned
+    with fg2_b200.Sim(n1, n2) as s:
+        s.config()
+        s.upload(x)
+        s.bcond()
+        s.kick(0.0, 0.0)
+        assert s.drift(dt / 3.0) == 0
+        assert np.array_equal(s.download(), out_mirror)
+    # ghost cell (-1, -1) after the periodic bcond is the image of interior cell (n1-1, n2-1)
+    assert np.array_equal(ghost, x[n1 - 1, n2 - 1])

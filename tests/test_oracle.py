@@ -137,3 +137,17 @@ def test_nan_input_flags_status():
     u = o.padded(x)
     v = o.empty(n1, n2)
     assert o.step(u, v, 0.0, 1e-3) == 1
+
+
+@pytest.mark.parametrize("name,shape,seed", [("kh", (300, 257), 2), ("noise", (64, 37), 1)])
+def test_numpy_setups_match_the_library(name, shape, seed):
+    """oracle/setups.py (the input of the bench's reference arm, which must not load the
+    product) gives the library's initial conditions to within one FP32 ulp."""
+    import fg2_b200
+    from oracle import setups
+    a = getattr(setups, name)(*shape, seed=seed)
+    b, _ = fg2_b200.setup_evaluate(name, shape[0], shape[1], seed=seed)
+    a32, b32 = a.astype(np.float32), b.astype(np.float32)
+    ulps = np.abs(a32.view(np.int32).astype(np.int64) - b32.view(np.int32).astype(np.int64))
+    assert ulps.max() <= 1
+    assert np.abs(a - b).max() <= 1e-15 * max(1.0, np.abs(b).max())
