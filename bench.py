@@ -205,10 +205,11 @@ def run_sweep_leg(device, steps=50, warmup=5):
             e1.synchronize()
             ms = e0.elapsed_time(e1) / steps
             status = s.sync()
-        rows.append({"n": n, "ms_per_step": ms, "gcell_steps_per_s": n * n / (ms / 1e3) / 1e9, "status": status,
-                     "reference_m2090_ms_per_step": ref_ms, "speedup_vs_reference": ref_ms / ms})
+        rows.append([n, ms, n * n / (ms / 1e3) / 1e9, status, ref_ms, ref_ms / ms])
     return {"workload": "hydro-isot FP32 periodic, noise sigma 0.01 seed 7, reference dt, "
-                        f"{steps} steps per size (the reference's bench/bench.txt sweep)", "rows": rows}
+                        f"{steps} steps per size (the reference's bench/bench.txt sweep)",
+            "columns": ["n", "ms_per_step", "gcell_steps_per_s", "status", "reference_m2090_ms_per_step",
+                        "speedup_vs_reference"], "rows": rows}
 
 
 def accuracy_vs_f64(scheme, n1, n2, x0, steps, dt, para=()):
@@ -374,6 +375,20 @@ def run_e2e(sim, state, stream, args, dist, device, world, cells):
 
 
 
+# ---- single-grid tiling -------------------------------------------------------------------
+def tune_single(sim, cache=None, key=None):
+    """Autotune a single grid's tiling (fg2_sim_autotune, state left unchanged), or apply the
+    tiling already found for the same key (grid size, scheme, storage).  Returns the tiling."""
+    if cache is not None and key in cache:
+        sim.set_tiling(*cache[key])
+        return cache[key]
+    sim.autotune(reps=3)
+    t = sim.tiling()
+    if cache is not None:
+        cache[key] = t
+    return t
+
+
 # ---- the batch path (secondary result) -----------------------------------------------------
 BATCH_SIDES = (64, 96, 128, 192, 256, 384, 512)
 BATCH_COUNT, BATCH_SEED = 512, 4
@@ -475,11 +490,13 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
     k_alone = min(steps, 20)
     alone_stream = torch.cuda.Stream(device=device)
     sims = []
+    tuned = {}
     for k, (n1, n2) in enumerate(sizes):
         s = fg2_b200.Sim(n1, n2, scheme="hydro-isot", stream=alone_stream.cuda_stream)
         s.set_box(two_pi, two_pi)
         s.config()
         s.upload(x0[k])
+        tune_single(s, tuned, (n1, n2))  # every grid size autotuned once
         s.set_time(0.0)
         s.advance(4, 0.0, graph=True)
         sims.append(s)
@@ -494,18 +511,24 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
         s.close()
     alone = cells * k_alone / (ms_alone / 1e3) / 1e9
     result["one_at_a_time"] = {"value": alone, "steps": k_alone, "ms_per_step": ms_alone / k_alone,
-                               "what": "same members, single-grid path, one simulation after another"}
+                               "what": "same members, single-grid path (tiling autotuned per grid size), "
+                                       "one simulation after another"}
     result["speedup_vs_one_at_a_time"] = value / alone
     return result
 
 
 # ---- the 16-bit deviation-storage path (secondary results) ----------------------------------
-B_ALG_F16 = 10 * NVAR * 2  # 80 B per cell-step: hydro, 16-bit u and v
+# 16-bit storage: u, v and the rounding residual r, 2 B per value.  Stage 0 reads u, r and
+# writes u', v, r; stage 1 reads u, v, r and writes u', v (its residual folded into v); stage 2
+# reads u, v and writes u', r: 14 array passes, 112 B per cell-step for hydro (80 B of them the
+# plain RK3 traffic of u and v, 32 B the compensation)
+B_ALG_F16 = 14 * NVAR * 2
 
 
 def run_mixed_leg(state, steps, warmup, device, plain_value):
     """The headline workload with the state stored as FP16 / BF16 deviations (per-field
-    background, per-64x64-tile scales), FP32 stencil, residual-carrying update."""
+    background, per-64x64-tile scales), FP32 stencil, compensated update (every rounding
+    residual kept)."""
     import torch
     import fg2_b200
     out = {}
@@ -514,6 +537,7 @@ def run_mixed_leg(state, steps, warmup, device, plain_value):
         sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=storage)
         sim.config()
         sim.upload(state)
+        tiling = tune_single(sim)
         sim.set_dt_mode("cfl")
         stream = torch.cuda.ExternalStream(sim.stream, device=device)
         sim.set_time(0.0)
@@ -531,7 +555,7 @@ def run_mixed_leg(state, steps, warmup, device, plain_value):
         sim.close()
         value = N1 * N2 * steps / (ms / 1e3) / 1e9
         out[storage] = {"value": value, "unit": "Gcell-steps/s", "ms_per_step": ms / steps, "status": status,
-                        "speedup_vs_plain_f32": value / plain_value,
+                        "speedup_vs_plain_f32": value / plain_value, "tiling": list(tiling),
                         "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_F16, "achieved": value * B_ALG_F16,
                                      "peak": peak, "unit": "GB/s", "frac": value * B_ALG_F16 / peak}}
     return out
@@ -580,12 +604,26 @@ def run_disk_leg(steps, warmup, device):
                          "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak}}
 
 
+def f16_numbers(x):
+    """The values of the FP16 numbers that deviation storage holds for the state x (per-field
+    mean as background, 0 for u2; per-64x64-tile largest deviation as scale), without their
+    rounding residual."""
+    n1, n2, nv = x.shape
+    bg = x.reshape(-1, nv).astype(np.float64).mean(0).astype(np.float32)
+    bg[2] = 0.0
+    t = 64
+    d = np.abs(x - bg).reshape(n1 // t, t, n2 // t, t, nv).max(axis=(1, 3))
+    d[~(d > 0)] = 1.0
+    s = np.repeat(np.repeat(d, t, 0), t, 1)
+    return (bg + s * ((x - bg) / s).astype(np.float16).astype(np.float32)).astype(np.float32)
+
+
 def run_precision_leg(n, steps, device):
     """Kelvin-Helmholtz at n x n, the same fixed step sequence in FP64, FP32 and the 16-bit
     deviation storages; per-field L2 (RMS) and Linf errors against the FP64 run, and the
     relative L2 error of the density rho = exp(lnd).  Also FP32 steps from the initial state
-    rounded once through FP16 deviation storage (`f32_from_f16_start`): the error that a single
-    16-bit rounding of the state leaves, whatever the update does afterwards."""
+    rounded once to the FP16 numbers of deviation storage, residual dropped (`f32_from_f16_start`):
+    the error that a single uncompensated 16-bit rounding of the state leaves."""
     import fg2_b200
     state = fg2_b200.setup_evaluate(SETUP, n, n, SCHEME, seed=SEED)[0]
     with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f64") as s:
@@ -600,10 +638,7 @@ def run_precision_leg(n, steps, device):
     rho_ref = np.exp(ref[..., 0])
     rho_norm = np.sqrt((rho_ref ** 2).sum())
     result = {"grid": [n, n], "steps": steps, "dt": dt, "fields": ["lnd", "u1", "u2", "lne"]}
-    with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f16") as s:
-        s.config()
-        s.upload(state32)
-        rounded_start = s.download()  # bg + s h: the state as FP16 deviation storage holds it
+    rounded_start = f16_numbers(state32)  # bg + s h: one FP16 rounding of the state, residual dropped
     for storage in ("f32", "f16", "bf16", "f32_from_f16_start"):
         with fg2_b200.Sim(n, n, scheme=SCHEME, storage="f32" if storage == "f32_from_f16_start" else storage) as s:
             s.config()
@@ -681,10 +716,12 @@ def run_combined_leg(device):
     # the plain FP32 path, one simulation after another on one stream
     stream = torch.cuda.Stream(device=device)
     sims = []
+    tuned = {}
     for k, (n1, n2) in enumerate(sizes):
         s = fg2_b200.Sim(n1, n2, scheme=SCHEME, storage="f32", stream=stream.cuda_stream)
         s.config()
         s.upload(states[k].astype(np.float32))
+        tune_single(s, tuned, (n1, n2))  # every grid size autotuned once
         s.advance(2, dt, graph=True)
         s.upload(states[k].astype(np.float32))
         sims.append(s)
@@ -709,10 +746,60 @@ def run_combined_leg(device):
             "f16_batch": {"value": v16, "unit": "Gcell-steps/s", "ms_per_step": ms16 / COMBINED_STEPS, "status": st16,
                           "rho_rel_l2_vs_f64": e16},
             "f32_one_at_a_time": {"value": v32, "unit": "Gcell-steps/s", "ms_per_step": ms32 / COMBINED_STEPS,
-                                  "status": st32, "rho_rel_l2_vs_f64": e32},
+                                  "status": st32, "rho_rel_l2_vs_f64": e32,
+                                  "tiling": {f"{k[0]}x{k[1]}": list(v) for k, v in tuned.items()}},
             "f32_batch": {"value": vb32, "unit": "Gcell-steps/s", "ms_per_step": msb32 / COMBINED_STEPS,
                           "status": stb32, "rho_rel_l2_vs_f64": eb32},
             "speedup": v16 / v32, "error_ratio": e16 / max(e32, 1e-300), "f64_status": st64}
+
+
+def compact(x, digits=5):
+    """Floats rounded to `digits` significant digits (the JSON line stays short)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}") if np.isfinite(x) else x
+    if isinstance(x, dict):
+        return {k: compact(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [compact(v, digits) for v in x]
+    return x
+
+
+def summary_of(line):
+    """The secondary legs' headline numbers in a few hundred bytes (the last key of the line,
+    so a truncated tail of the output still shows them)."""
+    def g(d, *keys):  # nested lookup, None where a level is missing
+        for k in keys:
+            d = d.get(k) if isinstance(d, dict) else None
+        return d
+
+    out = {}
+    out["plain_f32"] = {"gcs": line.get("value"), "hbm_frac": g(line, "roofline", "frac"),
+                        "e2e_gcs": g(line, "e2e", "value"), "tiling": [g(line, "tiling", "blocks_of_7_rows"),
+                                                                       g(line, "tiling", "ctas_per_sm")]}
+    if line.get("batch"):
+        b = line["batch"]
+        out["c4_batch"] = {"gcs": b.get("value"), "hbm_frac": g(b, "roofline", "frac"),
+                           "one_at_a_time_gcs": g(b, "one_at_a_time", "value")}
+    if line.get("mixed"):
+        out["mixed_4096"] = {k: {"gcs": v.get("value"), "x_f32": v.get("speedup_vs_plain_f32")}
+                             for k, v in line["mixed"].items()}
+    if line.get("precision"):
+        p = line["precision"]
+        out["c3_rho_rel_l2"] = {k: g(p, k, "rho_rel_l2") for k in ("f32", "f16", "bf16", "f32_from_f16_start")}
+    if line.get("combined"):
+        c = line["combined"]
+        out["c5"] = {"f16_batch_gcs": g(c, "f16_batch", "value"), "f32_alone_gcs": g(c, "f32_one_at_a_time", "value"),
+                     "f32_batch_gcs": g(c, "f32_batch", "value"), "speedup": c.get("speedup"),
+                     "rho_err_ratio": c.get("error_ratio")}
+    if line.get("disk"):
+        out["disk_gcs"] = line["disk"].get("value")
+    if line.get("small"):
+        out["c1"] = {"gpu_gcs": g(line, "small", "gpu", "value"), "cpu_gcs": g(line, "small", "cpu", "value")}
+    if line.get("sweep"):
+        cols = line["sweep"]["columns"]
+        out["sweep_gcs"] = {str(r[0]): r[cols.index("gcell_steps_per_s")] for r in line["sweep"]["rows"]}
+    out["cpu_baseline_gcs"] = g(line, "cpu_baseline", "value")
+    return compact(out, 4)
 
 
 def run_fused(args):
@@ -747,11 +834,15 @@ def run_fused(args):
     dist = dist_init(world, "nccl")
 
     sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=args.storage)
-    elem = 2 if args.storage in ("f16", "bf16") else 4
-    b_alg = B_ALG * elem // ELEM  # 160 B per cell-step in FP32, 80 B with 16-bit storage
+    b_alg = B_ALG_F16 if args.storage in ("f16", "bf16") else B_ALG  # 160 B FP32, 112 B 16-bit
     sim.config()
     state = initial_state()
     sim.upload(state)
+    if args.tiling:  # fixed tiling (profiling runs: no autotune launches before the captured ones)
+        sim.set_tiling(*[int(x) for x in args.tiling.split(",")])
+        tiling = sim.tiling()
+    else:
+        tiling = tune_single(sim)  # the successor of the reference's block-size heuristic
     sim.set_dt_mode("cfl")
     stream = torch.cuda.ExternalStream(sim.stream, device=device)
     cells = N1 * N2
@@ -850,6 +941,8 @@ def run_fused(args):
                          "frac_nominal_8tbs": achieved / 8000.0,
                          "bytes_per_cell_step": b_alg, "stage_ms": stage_ms},
             "step_hbm_frac": value / world * b_alg / peak,
+            "tiling": {"blocks_of_7_rows": tiling[0], "ctas_per_sm": tiling[1], "strip_columns": 128,
+                       "how": "--tiling" if args.tiling else "fg2_sim_autotune on the workload's own state"},
             "cpu_baseline": cpu,
             "accuracy_vs_f64": accuracy,
             "e2e": e2e, "e2e_status": e2e_status,
@@ -863,7 +956,8 @@ def run_fused(args):
             "gpu_launches": 4 * args.steps,
             "clocks": clk.summary(),
         }
-        print(json.dumps(line), flush=True)
+        line["summary"] = summary_of(line)
+        print(json.dumps(compact(line)), flush=True)
     sim.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -889,6 +983,8 @@ def main():
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
+    ap.add_argument("--tiling", default="",
+                    help="nb,ctas_per_sm of the headline workload's launches (default: autotune)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
                     help="state storage of the headline workload (f16/bf16: deviation storage)")
     args = ap.parse_args()

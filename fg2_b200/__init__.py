@@ -44,6 +44,8 @@ def _bind(lib):
         "fg2_sim_create": (P, [I, I, I, P]), "fg2_sim_destroy": (None, [P]),
         "fg2_sim_device_bytes": (SZ, [P]), "fg2_sim_storage": (I, [P]),
         "fg2_sim_set_box": (I, [P, D, D]), "fg2_sim_set_courant": (I, [P, D]), "fg2_sim_set_tiling": (I, [P, I]),
+        "fg2_sim_set_occupancy": (I, [P, I]), "fg2_sim_get_tiling": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "fg2_sim_autotune": (I, [P, I, ctypes.POINTER(D)]),
         "fg2_sim_set_bcond": (I, [P, I, I]), "fg2_sim_para": (S, [P, S]),
         "fg2_sim_get_para": (I, [P, S, ctypes.POINTER(D)]), "fg2_sim_config": (I, [P]),
         "fg2_sim_init": (I, [P, S, U64]), "fg2_sim_upload": (I, [P, P]), "fg2_sim_download": (I, [P, P]),
@@ -176,9 +178,25 @@ class Sim:
     def set_courant(self, c):
         self._check(self.lib.fg2_sim_set_courant(self.h, c), "set_courant")
 
-    def set_tiling(self, nb):
-        """Tile height of the fused kernel in blocks of 7 rows (0: the default)."""
+    def set_tiling(self, nb, ctas_per_sm=None):
+        """Tile height of the fused kernel in blocks of 7 rows (0: the default) and, if given,
+        CTAs per SM of its persistent grid (0: as many as fit)."""
         self._check(self.lib.fg2_sim_set_tiling(self.h, int(nb)), "set_tiling")
+        if ctas_per_sm is not None:
+            self._check(self.lib.fg2_sim_set_occupancy(self.h, int(ctas_per_sm)), "set_occupancy")
+
+    def tiling(self):
+        """(tile height in blocks of 7 rows, CTAs per SM) the launches use."""
+        nb, c = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.fg2_sim_get_tiling(self.h, ctypes.byref(nb), ctypes.byref(c)), "tiling")
+        return nb.value, c.value
+
+    def autotune(self, reps=3):
+        """Time every tiling candidate on this simulation's state (left unchanged) and keep the
+        fastest; returns its ms per step."""
+        ms = ctypes.c_double()
+        self._check(self.lib.fg2_sim_autotune(self.h, int(reps), ctypes.byref(ms)), "autotune")
+        return ms.value
 
     def set_bcond(self, p1, p2):
         self._check(self.lib.fg2_sim_set_bcond(self.h, int(p1), int(p2)), "set_bcond")

@@ -34,6 +34,15 @@ def lib_path(scheme):
     return os.path.join(LIB, f"libfg2_{scheme}.so")
 
 
+def _headers(scheme):
+    """Headers every source of `scheme` may include."""
+    out = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    sdir = os.path.join(CSRC, "schemes", scheme)
+    out += [os.path.join(sdir, f) for f in os.listdir(sdir)]
+    out.append(os.path.join(os.path.dirname(HERE), "include", "fg2_b200.h"))
+    return out
+
+
 def _deps():
     out = []
     for root, _, files in os.walk(CSRC):
@@ -49,8 +58,14 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _obj(scheme, src):
+    return os.path.join(BUILD, scheme, src + ".o")
+
+
 def _compile(scheme, src):
-    obj = os.path.join(BUILD, scheme, src + ".o")
+    obj = _obj(scheme, src)
+    if not _stale(obj, [os.path.join(CSRC, src)] + _headers(scheme)):
+        return obj  # up to date
     os.makedirs(os.path.dirname(obj), exist_ok=True)
     cmd = [nvcc(), *NVCC_FLAGS, "-I", CSRC, "-I", os.path.join(CSRC, "schemes", scheme),
            "-x", "cu" if src.endswith(".cu") else "c++", "-c", os.path.join(CSRC, src), "-o", obj]

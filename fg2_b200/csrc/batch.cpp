@@ -142,7 +142,7 @@ int enqueue_batch_step(fg2_batch *b, double dt, bool device_dt, double t_end, in
     a.strip = b->strip;
     a.reverse = b->reverse;
     b->reverse ^= 1;
-    a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
+    a.comp_bg = k == 1 ? RK_BETA[2] * RK_GAMMA[2] : 0.0;  // 16-bit stage 1 folds its residual into v
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
     CK(launch_substage(b->storage, kind, device_dt && k == 2, true, b->desc + (size_t)set * b->count, b->count,
                        b->ntiles, a, b->queue, b->stream));
@@ -247,7 +247,7 @@ fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage
   for (int k = 0; k < count; ++k) {
     const Layout L = make_layout(n1[k], n2[k], scheme::NVAR);
     bytes[k] = align_up((size_t)L.elems() * elem, 256);
-    b->arena_bytes += 3 * bytes[k];
+    b->arena_bytes += arrays_per_sim(storage) * bytes[k];
     b->cells += (long long)n1[k] * n2[k];
   }
   if (cudaMalloc(&b->arena, b->arena_bytes) != cudaSuccess || cudaMalloc(&b->status, count * sizeof(Status)) != cudaSuccess ||
@@ -267,12 +267,18 @@ fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage
   }
   std::memset(b->status_host, 0, count * sizeof(Status));
   char *p = (char *)b->arena;
+  const int na = arrays_per_sim(storage);
   for (int k = 0; k < count; ++k) {
-    fg2_sim *m = sim_create_in(n1[k], n2[k], storage, b->stream, p, p + bytes[k], p + 2 * bytes[k], &b->status[k],
+    void *r = na > 3 ? p + 3 * bytes[k] : nullptr;  // 16-bit storage: the rounding residual
+    if (r && cudaMemsetAsync(r, 0, bytes[k], b->stream) != cudaSuccess) {
+      fail(FG2_ERR_ALLOC, "initial fill of the batch failed");
+      return nullptr;
+    }
+    fg2_sim *m = sim_create_in(n1[k], n2[k], storage, b->stream, p, p + bytes[k], p + 2 * bytes[k], r, &b->status[k],
                                &b->status_host[k]);
     if (!m) return nullptr;
     b->members.push_back(m);
-    p += 3 * bytes[k];
+    p += na * bytes[k];
   }
   b->order.resize(count);
   for (int k = 0; k < count; ++k) b->order[k] = k;
@@ -495,6 +501,16 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
       for (int warps : {0, 4, 8, 12})
         cands.push_back({strip, nb, warps * 32 / strip, std::numeric_limits<double>::infinity()});
   const int keep_nb = b->nb, keep_ctas = b->max_ctas, keep_strip = b->strip;
+  // 16-bit storage: a step of dt = 0 re-encodes the state and drops its rounding residual, so
+  // the members' arrays are kept aside and put back afterwards
+  void *keep = nullptr;
+  if (b->members[0]->dev_storage) {
+    CK(cudaMalloc(&keep, b->arena_bytes));
+    CK(cudaMemcpyAsync(keep, b->arena, b->arena_bytes, cudaMemcpyDeviceToDevice, b->stream));
+  }
+  std::unique_ptr<void, cudaError_t (*)(void *)> hold(keep, cudaFree);
+  std::vector<int> keep_cur;
+  for (fg2_sim *m : b->members) keep_cur.push_back(m->cur);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -526,6 +542,11 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (keep) {
+    CK(cudaMemcpyAsync(b->arena, keep, b->arena_bytes, cudaMemcpyDeviceToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    for (size_t k = 0; k < b->members.size(); ++k) b->members[k]->cur = keep_cur[k];
+  }
   b->strip = rc ? keep_strip : cands[0].strip;
   b->nb = rc ? keep_nb : cands[0].nb;
   b->max_ctas = rc ? keep_ctas : cands[0].ctas;

@@ -117,12 +117,19 @@ enum ErrorBits : unsigned { ERR_TMA_TIMEOUT = 1u, ERR_QUEUE_TIMEOUT = 2u };
 // images).  Fields whose sign flips at a reflecting wall have bg = 0, so a ghost image is the
 // negated 16-bit number.  v (the RK3 register) is stored as plain 16-bit numbers.
 constexpr int SCALE_TILE = 64;
+//
+// The state is kept exactly as S - e, S the stored number's value and e the rounding error of
+// the encode that produced it (the residual, the low part of a two-sum).  e is stored in the
+// array r (same layout as v, interior cells only) as the 16-bit number e / s * RESID_SCALE:
+// |e| <= s 2^-12 for FP16 numbers |h| <= 1, so the stored residual is at most about 1.
 constexpr int DEV_MAX_FIELDS = 4;  // the codes hold one background and scale per field
+constexpr double RESID_SCALE = 4096.0;
 struct DevCode {
   float bg[4];           // per-field background (field mean at upload)
   const float4 *scale;   // per tile, row-major over (n1 / 64, n2 / 64) tiles: s of each field
   const float4 *inv;     // per tile: 1 / s
   int tiles2;            // tiles along axis 2
+  void *r;               // rounding residual of the state (16-bit numbers, layout of v)
 };
 
 // ---- arithmetic on a scalar or on a pair of cells ------------------------------------------

@@ -273,6 +273,12 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   const int G = group_cells(storage), vbw = (sw + GL % G + G - 1) / G * G;
   r = encode_map(&d->tm_v, v, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
+  if (dev && dev->r) {
+    r = encode_map(&d->tm_r, dev->r, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+    if (r != CUDA_SUCCESS) return r;
+  } else {
+    d->tm_r = d->tm_v;  // never read: only 16-bit stages load r
+  }
   d->u_out = u_out;
   d->v = v;
   d->L = L;
@@ -290,7 +296,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   d->delta1 = delta1;
   d->delta2 = delta2;
   if (dev) d->dev = *dev;
-  else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0};
+  else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0, nullptr};
   return CUDA_SUCCESS;
 }
 
@@ -305,7 +311,7 @@ template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC, int
 static cudaError_t run_substage_w(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
                                   int max_ctas, int *queue, cudaStream_t s)
 {
-  using G = sub::Geo<S, RV, W>;
+  using G = sub::Geo<S, RV, Store<S>::DEV && WU && WV, W>;  // 16-bit stages 0 and 1 also load r
   auto kern = sub::substage_kernel<S, M2, RV, WV, WU, CF, SC, W>;
   static int ctas_per_sm = 0, sms = 0;
   if (!ctas_per_sm) {
@@ -470,7 +476,8 @@ __global__ void fill_kernel(T *p, size_t n, T x)
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) p[k] = x;
 }
 
-// Value of field f at interior cell (i, j), decoded for 16-bit deviation storage.
+// Value of field f at interior cell (i, j), decoded for 16-bit deviation storage: the stored
+// number's value S = bg + s h less the rounding residual e = s r / RESID_SCALE.
 template <class S>
 __device__ __forceinline__ double value_at(const S *u, const Layout &L, const DevCode &dc, int f, int i, int j)
 {
@@ -479,7 +486,10 @@ __device__ __forceinline__ double value_at(const S *u, const Layout &L, const De
   } else {
     const float4 sc = __ldg(dc.scale + (i / SCALE_TILE) * dc.tiles2 + j / SCALE_TILE);
     const float sf = f == 0 ? sc.x : f == 1 ? sc.y : f == 2 ? sc.z : sc.w;
-    return (double)fmaf(sf, Store<S>::to(u[L.at(f, i, j)]), dc.bg[f]);
+    const double x = (double)fmaf(sf, Store<S>::to(u[L.at(f, i, j)]), dc.bg[f]);
+    if (!dc.r) return x;
+    const double e = (double)Store<S>::to(reinterpret_cast<const S *>(dc.r)[L.at(f, i, j)]) * (double)sf / RESID_SCALE;
+    return x - e;
   }
 }
 
@@ -586,9 +596,17 @@ __global__ void encode_kernel(S *u, const float *src, const Layout L, const DevC
       u[L.at(f, i, j)] = Store<S>::from(src[k]);
       continue;
     }
-    const float4 iv = __ldg(dc.inv + (i / SCALE_TILE) * dc.tiles2 + j / SCALE_TILE);
+    const int t = (i / SCALE_TILE) * dc.tiles2 + j / SCALE_TILE;
+    const float4 iv = __ldg(dc.inv + t), sc = __ldg(dc.scale + t);
     const float inv = f == 0 ? iv.x : f == 1 ? iv.y : f == 2 ? iv.z : iv.w;
-    u[L.at(f, i, j)] = Store<S>::from((src[k] - dc.bg[f]) * inv);
+    const float sf = f == 0 ? sc.x : f == 1 ? sc.y : f == 2 ? sc.z : sc.w;
+    const S h = Store<S>::from((src[k] - dc.bg[f]) * inv);
+    u[L.at(f, i, j)] = h;
+    // the rounding residual e = S - x, kept as e / s * RESID_SCALE (the substage's encoding)
+    if (dc.r) {
+      const float e = fmaf(sf, Store<S>::to(h), dc.bg[f]) - src[k];
+      reinterpret_cast<S *>(dc.r)[L.at(f, i, j)] = Store<S>::from(e * (inv * (float)RESID_SCALE));
+    }
   }
 }
 

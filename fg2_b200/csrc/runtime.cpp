@@ -9,6 +9,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -114,9 +115,10 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p1 = s->p1;
   a.p2 = s->p2;
   a.status = s->status;
-  a.comp_bg = k < 2 ? RK_BETA[k + 1] * RK_GAMMA[k + 1] : 0.0;
+  a.comp_bg = k == 1 ? RK_BETA[2] * RK_GAMMA[2] : 0.0;  // 16-bit stage 1 folds its residual into v
   a.wait_test_bytes = s->wait_test_bytes;
   a.nb = tile_height(s);
+  a.max_ctas = s->max_ctas;
   return a;
 }
 
@@ -429,8 +431,8 @@ fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_a
 
 }  // namespace
 
-fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, Status *status,
-                       Status *status_host)
+fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r,
+                       Status *status, Status *status_host)
 {
   fg2_sim *s = new_handle(n1, n2, storage, stream, false);
   if (!s) return nullptr;
@@ -439,8 +441,14 @@ fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u
   s->v = v;
   s->status = status;
   s->status_host = status_host;
+  if (s->dev_storage) {
+    s->r = r;
+    s->dev.r = r;
+  }
   return s;
 }
+
+int arrays_per_sim(int storage) { return storage == ST_F16 || storage == ST_BF16 ? 4 : 3; }
 
 }  // namespace rt
 }  // namespace fg2
@@ -454,10 +462,11 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (!s) return nullptr;
   const size_t bytes = array_elems(s.get()) * elem_size(storage);
   if (cudaMalloc(&s->u[0], bytes) != cudaSuccess || cudaMalloc(&s->u[1], bytes) != cudaSuccess ||
-      cudaMalloc(&s->v, bytes) != cudaSuccess) {
+      cudaMalloc(&s->v, bytes) != cudaSuccess || (s->dev_storage && cudaMalloc(&s->r, bytes) != cudaSuccess)) {
     fail(FG2_ERR_ALLOC, "device allocation of the state failed");
     return nullptr;
   }
+  s->dev.r = s->r;  // null unless 16-bit storage
   if (cudaMalloc(&s->status, sizeof(Status)) != cudaSuccess ||
       cudaMallocHost(&s->status_host, sizeof(Status)) != cudaSuccess) {
     fail(FG2_ERR_ALLOC, "status allocation failed");
@@ -468,6 +477,7 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->u[1], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->v, array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
+      (s->r && cudaMemsetAsync(s->r, 0, bytes, s->stream) != cudaSuccess) ||
       cudaMemsetAsync(s->status, 0, sizeof(Status), s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess) {
     fail(FG2_ERR_ALLOC, "initial fill failed");
@@ -485,6 +495,7 @@ void fg2_sim_destroy(fg2_sim *s)
     cudaFree(s->u[0]);
     cudaFree(s->u[1]);
     cudaFree(s->v);
+    cudaFree(s->r);
     cudaFree(s->status);
     cudaFreeHost(s->status_host);
   }
@@ -498,7 +509,10 @@ void fg2_sim_destroy(fg2_sim *s)
   delete s;
 }
 
-size_t fg2_sim_device_bytes(const fg2_sim *s) { return s ? 3 * array_elems(s) * elem_size(s->storage) : 0; }
+size_t fg2_sim_device_bytes(const fg2_sim *s)
+{
+  return s ? arrays_per_sim(s->storage) * array_elems(s) * elem_size(s->storage) : 0;
+}
 int fg2_sim_storage(const fg2_sim *s) { return s ? s->storage : -1; }
 
 int fg2_sim_set_box(fg2_sim *s, double l1, double l2)
@@ -517,6 +531,97 @@ int fg2_sim_set_tiling(fg2_sim *s, int nb)
   if (nb != s->nb) drop_graph(s);
   s->nb = nb;
   return FG2_OK;
+}
+
+int fg2_sim_set_occupancy(fg2_sim *s, int ctas_per_sm)
+{
+  if (!s || ctas_per_sm < 0 || ctas_per_sm > 64) return fail(FG2_ERR_ARG, "bad occupancy %d", ctas_per_sm);
+  if (ctas_per_sm != s->max_ctas) drop_graph(s);
+  s->max_ctas = ctas_per_sm;
+  return FG2_OK;
+}
+
+int fg2_sim_get_tiling(const fg2_sim *s, int *nb, int *ctas_per_sm)
+{
+  if (!s) return fail(FG2_ERR_ARG, "null handle");
+  if (nb) *nb = tile_height(s);
+  if (ctas_per_sm) *ctas_per_sm = s->max_ctas;
+  return FG2_OK;
+}
+
+int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
+{
+  if (!s || reps < 1) return fail(FG2_ERR_ARG, "bad arguments");
+  ensure_config(s);
+  struct Cand {
+    int nb, ctas;
+    double ms;
+  };
+  std::vector<Cand> cands;
+  // tile height nb blocks of 7 rows; CTAs per SM: 0 = as many as fit, or 4, 8, 12 warps
+  for (int nb : {1, 2, 3, 4, 5, 6, 8})
+    for (int warps : {0, 4, 8, 12}) cands.push_back({nb, warps * 32 / STRIP_DEFAULT, 0.0});
+  const int keep_nb = s->nb, keep_ctas = s->max_ctas, keep_cur = s->cur;
+  const bool keep_ghosts = s->ghosts_valid, keep_smax = s->smax_valid;
+  // 16-bit storage: a step of dt = 0 re-encodes the state and drops its rounding residual, so
+  // the state and the residual are kept aside and put back afterwards
+  const size_t bytes = array_elems(s) * elem_size(s->storage);
+  void *keep = nullptr;
+  if (s->dev_storage) {
+    CK(cudaMalloc(&keep, 2 * bytes));
+    CK(cudaMemcpyAsync(keep, s->u[s->cur], bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync((char *)keep + bytes, s->r, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  std::unique_ptr<void, cudaError_t (*)(void *)> hold(keep, cudaFree);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto measure = [&](Cand &c) -> int {
+    s->nb = c.nb;
+    s->max_ctas = c.ctas;
+    int r = FG2_OK;
+    // two untimed steps, then 2 reps timed (dt = 0: u' = u + 0 v, bitwise)
+    for (int q = 0; q < 2 && r == 0; ++q) r = enqueue_step(s, 0.0, nullptr, false);
+    if (r) return r;
+    if (cudaEventRecord(e0, s->stream) != cudaSuccess) return fail(FG2_ERR_ARG, "event record failed");
+    for (int q = 0; q < 2 * reps && r == 0; ++q) r = enqueue_step(s, 0.0, nullptr, false);
+    if (r) return r;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, s->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return fail(FG2_ERR_ARG, "autotune timing failed");
+    c.ms = ms / (2.0 * reps);
+    return FG2_OK;
+  };
+  int rc = FG2_OK;
+  for (size_t i = 0; i < cands.size() && rc == 0; ++i) rc = measure(cands[i]);
+  if (rc == 0) {  // the three best again, each scored by its faster measurement
+    std::sort(cands.begin(), cands.end(), [](const Cand &x, const Cand &y) { return x.ms < y.ms; });
+    for (size_t i = 0; i < 3 && i < cands.size() && rc == 0; ++i) {
+      const double first = cands[i].ms;
+      rc = measure(cands[i]);
+      cands[i].ms = std::min(first, cands[i].ms);
+    }
+    std::sort(cands.begin(), cands.end(), [](const Cand &x, const Cand &y) { return x.ms < y.ms; });
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (keep) {
+    CK(cudaMemcpyAsync(s->u[keep_cur], keep, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->r, (char *)keep + bytes, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  // every stage of dt = 0 copied the state bitwise into the array it wrote, ghost images
+  // included, so both arrays hold it; 16-bit storage got its own arrays back
+  s->cur = keep_cur;
+  s->ghosts_valid = s->dev_storage ? keep_ghosts : true;
+  s->smax_valid = keep_smax;  // the state is unchanged
+  s->nb = rc ? keep_nb : cands[0].nb;
+  s->max_ctas = rc ? keep_ctas : cands[0].ctas;
+  drop_graph(s);
+  if (rc) return rc;
+  if (best_ms) *best_ms = cands[0].ms;
+  return read_status(s);
 }
 
 int fg2_sim_set_courant(fg2_sim *s, double c)

@@ -34,6 +34,7 @@ struct fg2_sim {
   unsigned version = 0;       // bumped whenever settings that descriptors depend on change
   int order = 0;              // tile order of the next substage launch (alternates)
   int nb = 0;                 // tile height in blocks of 7 rows (0: the default)
+  int max_ctas = 0;           // CTAs per SM of the persistent grid (0: as many as fit)
   unsigned wait_test_bytes = 0;  // timeout-path tests (fg2_sim_test_stall_waits)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;
@@ -59,6 +60,7 @@ struct fg2_sim {
   bool dev_storage = false;
   int tiles1 = 0, tiles2 = 0;
   float4 *scale_dev = nullptr, *inv_dev = nullptr;
+  void *r = nullptr;  // rounding residual of the state (16-bit numbers, layout of v)
   fg2::DevCode dev{};
 };
 
@@ -86,10 +88,13 @@ int read_status(fg2_sim *s);
 // The handle's deviation codes for kernels that decode the state (null: plain storage).
 const fg2::DevCode *dev_code(const fg2_sim *s);
 void drop_graph(fg2_sim *s);
-// A handle over caller-owned device memory: arrays u0, u1, v of the handle's layout and one
-// status block (device) with its pinned host mirror; the handle frees none of them.
-fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v,
+// A handle over caller-owned device memory: arrays u0, u1, v (and, for 16-bit storage, the
+// residual r, zero-filled) of the handle's layout and one status block (device) with its
+// pinned host mirror; the handle frees none of them.
+fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r,
                        Status *status, Status *status_host);
+// Arrays per simulation in device memory: u[0], u[1], v, and r for 16-bit storage.
+int arrays_per_sim(int storage);
 
 }  // namespace rt
 }  // namespace fg2

@@ -88,11 +88,13 @@ __host__ __device__ constexpr int group_of(int elem)
   return ((elem >= 8 ? 2 : 4) * NV * elem) % 16 == 0 ? (elem >= 8 ? 2 : 4) : 2 * (elem >= 8 ? 2 : 4);
 }
 
-// Shared memory of one CTA: NSLOT slots of [u box | v box] (the v box only when the stage
-// reads v), the FP32 copy of the landed u box (deviation storage), then the mbarriers and
-// the producer's bookkeeping.  The v box starts VOFF cells left of the strip when a cell
-// group is wider than the 4 ghost columns.
-template <class S, bool RV, int W>
+// Shared memory of one CTA: NSLOT slots of [u box | v box | r box] (the v box only when the
+// stage reads v, the r box only when it reads the rounding residual of 16-bit storage), two
+// FP32 copies of a landed u box (deviation storage: chunk n is stenciled from one while chunk
+// n + 1 is decoded into the other), then the mbarriers and the producer's bookkeeping.  The
+// v and r boxes start VOFF cells left of the strip when a cell group is wider than the 4
+// ghost columns.
+template <class S, bool RV, bool RR, int W>
 struct Geo {
   static constexpr int SW = Strip<W>::SW, BW = Strip<W>::BW;
   static constexpr bool DEV = Store<S>::DEV;
@@ -104,10 +106,13 @@ struct Geo {
   static constexpr uint32_t U_BYTES = (uint32_t)(BW * CH * CB);
   static constexpr uint32_t V_OFF = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
   static constexpr uint32_t V_BYTES = (uint32_t)(VBW * CH * CB);
-  static constexpr uint32_t SLOT = V_OFF + (RV ? (V_BYTES + 127) / 128 * 128 : 0);
+  static constexpr uint32_t V_AL = (V_BYTES + 127) / 128 * 128;
+  static constexpr uint32_t R_OFF = V_OFF + (RV ? V_AL : 0);
+  static constexpr uint32_t SLOT = R_OFF + (RR ? V_AL : 0);
   static constexpr size_t DEC_OFF = (size_t)NSLOT * SLOT;
-  static constexpr size_t DEC_BYTES = DEV ? (size_t)BW * CH * NV * sizeof(float) : 0;
-  static constexpr size_t BAR_OFF = DEC_OFF + (DEC_BYTES + 127) / 128 * 128;
+  static constexpr size_t DEC_ONE = DEV ? ((size_t)BW * CH * NV * sizeof(float) + 127) / 128 * 128 : 0;
+  static constexpr size_t DEC_BYTES = 2 * DEC_ONE;
+  static constexpr size_t BAR_OFF = DEC_OFF + DEC_BYTES;
   // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
   static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
@@ -280,8 +285,9 @@ struct GridRegs {
   T s12, inv1, inv2, delta1, delta2;  // 1/(Delta1 Delta2), CFL factors, Delta1, Delta2
   // deviation storage
   P bg[NP];                    // per-field background
-  P comp;                      // 1 / (beta' gamma' dt) of the next stage, or 0
+  P comp;                      // -1 / (beta' gamma' dt) of the next stage (stage 1), or 0
   const float4 *scale, *inv;   // per-tile s and 1/s
+  S *r;                        // rounding residual array
   int tiles2;
 };
 
@@ -498,10 +504,19 @@ __device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, 
 }
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
-// vr is v of the cell (read stages), cg the scheme's geometry of the thread's column.  u' and
-// v go straight to HBM; edge cells also write their ghost images.
+// vr is v of the cell (read stages), rr its rounding residual (16-bit stages 0 and 1), tj the
+// scale-tile column of the thread's column, cg the scheme's geometry of the column.  u' and v
+// go straight to HBM; edge cells also write their ghost images.
+//
+// Deviation storage keeps the state exactly as the 16-bit number S plus a residual: the value
+// is T = S - e with e the rounding error of the last encode.  Stages 0 and 1 read e (scaled by
+// 1 / s and RESID_SCALE, stored as a 16-bit number in r) and update T instead of S, so every
+// rounding is compensated (the two-sum u' = T + gamma dt v = S' - e').  Stage 0's and stage 2's
+// e' go to r; stage 1's e' is folded into v (stored as v - e' / (beta2 gamma2 dt)), which stage
+// 2 reads once, with no carry beyond it.  The stencil itself reads S.
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
+__device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP],
+                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j, int tj,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
                                          const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
                                          typename Store<S>::C &rate, const scheme::Geom<typename Store<S>::C> &cg)
@@ -509,6 +524,10 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
   using St = Store<S>;
+  constexpr bool DEV = St::DEV;
+  constexpr bool RR = DEV && WRITE_U && WRITE_V;                 // stages 0 and 1
+  constexpr bool WR = DEV && WRITE_U && !(READ_V && WRITE_V);    // stages 0 and 2
+  constexpr bool FOLD = DEV && WRITE_U && READ_V && WRITE_V;     // stage 1
   constexpr int S0 = (R + 4) % CH;
   Cell<T, NV> cell;
   emit_pair<T, M2, SC, S0, 0>(a, gr, s, cell);
@@ -522,38 +541,52 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   const T dl1 = SC ? gr.delta1 : a.ks.delta1, dl2 = SC ? gr.delta2 : a.ks.delta2;
   scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2, cg);
   if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
+  P sc[NP], iv[NP];  // deviation storage: the scales of the cell's tile
+  if constexpr (DEV && WRITE_U) {
+    const int t = (i >> 6) * gr.tiles2 + tj;  // SCALE_TILE = 64
+    const float4 x = __ldg(gr.scale + t), y = __ldg(gr.inv + t);
+    sc[0] = make_float2(x.x, x.y);
+    iv[0] = make_float2(y.x, y.y);
+    if constexpr (NP > 1) {
+      sc[NP - 1] = make_float2(x.z, x.w);
+      iv[NP - 1] = make_float2(y.z, y.w);
+    }
+  }
   P vn[NP], qp[NP];
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
     vn[p] = PairOf<T>::make(r[2 * p], 2 * p + 1 < NV ? r[2 * p + 1] : T(0));
     if (READ_V) vn[p] = fmac(a.beta2, vr[p], vn[p]);
-    qp[p] = fmac(gr.gdt, vn[p], s.w[p][S0]);
+    P base = s.w[p][S0];
+    if constexpr (RR) base = fmac(rr[p], sc[p] * lit<P>(-1.0 / RESID_SCALE), base);  // T = S - e
+    qp[p] = fmac(gr.gdt, vn[p], base);
   }
   const long long o = gr.L.at(0, i, j);
-  if constexpr (!St::DEV) {
+  if constexpr (!DEV) {
     if (WRITE_U) store_cell<S>(gr.u_out + o, qp);
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
   S raw[NV];
-  if constexpr (St::DEV) {
+  if constexpr (DEV) {
     if (WRITE_U) {
-      // encode u' with its tile's 1/s; the residual of the rounding goes into v
-      const int t = (i / SCALE_TILE) * gr.tiles2 + j / SCALE_TILE;
-      const float4 iv = __ldg(gr.inv + t);
-      const P ivp[2] = {make_float2(iv.x, iv.y), make_float2(iv.z, iv.w)};
-      P h[NP], hs[NP];
+      // encode u' with its tile's 1/s; e' = S' - u' is the rounding residual
+      P h[NP], hs[NP], e[NP];
 #pragma unroll
-      for (int p = 0; p < NP; ++p) h[p] = (qp[p] - gr.bg[p]) * ivp[p];
+      for (int p = 0; p < NP; ++p) h[p] = (qp[p] - gr.bg[p]) * iv[p];
       encode_cell<S>(gr.u_out + o, h, hs, raw);
-      if (WRITE_V) {
-        const float4 sc = __ldg(gr.scale + t);
-        const P scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
 #pragma unroll
-        for (int p = 0; p < NP; ++p) vn[p] = vn[p] - (fmac(scp[p], hs[p], gr.bg[p]) - qp[p]) * gr.comp;
+      for (int p = 0; p < NP; ++p) e[p] = fmac(sc[p], hs[p], gr.bg[p]) - qp[p];
+      if constexpr (FOLD) {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) vn[p] = fmac(e[p], gr.comp, vn[p]);
+      }
+      if constexpr (WR) {
+        P ro[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) ro[p] = e[p] * (iv[p] * lit<P>(RESID_SCALE));
+        store_cell<S>(gr.r + o, ro);
       }
     }
-  }
-  if constexpr (St::DEV) {
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
   if (WRITE_U) {
@@ -566,7 +599,7 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
     for (int f = 1; f < NV; ++f) sum += qn[f];
     nan |= sum != sum;
     if (rim) {  // tiles within HALF cells of an edge: the cell's ghost images for the next stage
-      if constexpr (!St::DEV) {
+      if constexpr (!DEV) {
         if constexpr (NP == 3) rim_images3<S>(gr.u_out, gr.L, i, j, qp[0], qp[1], qp[2], gr.p1, gr.p2);
         else rim_images<S>(gr.u_out, gr.L, i, j, qp[0], qp[NP - 1], gr.p1, gr.p2);
       }
@@ -602,12 +635,12 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 // `claim` (a register of the issuing thread) holds the queue position of the CTA's next tile:
 // it is drawn when the last chunk of the current tile is issued, one chunk before it is
 // needed, so the atomic's round trip is off the chunk's critical path.
-template <class S, bool READ_V, int W>
+template <class S, bool READ_V, bool READ_R, int W>
 __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
                                             int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
                                             bool reverse, unsigned extra_bytes, int *queue, int &claim)
 {
-  using G = Geo<S, READ_V, W>;
+  using G = Geo<S, READ_V, READ_R, W>;
   if (ps->done) return;
   const int n = ps->next_n, s = n % G::NSLOT;
   if (ps->c == 0) {
@@ -631,14 +664,18 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
   } else {
     const GridDesc &gd = grids[ps->g];
     const int i0 = ps->i0, j0 = ps->j0, c = ps->c;
-    const bool with_v = READ_V && c > 0;
-    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + extra_bytes);
+    const bool with_v = READ_V && c > 0, with_r = READ_R && c > 0;
+    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + (with_r ? G::V_BYTES : 0u) + extra_bytes);
     // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
     // columns j0 - 4 .. (padded column j0)
     tma_load_3d(smem + (size_t)s * G::SLOT, &gd.tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
     // v of the 7 output rows of block c - 1
     if (with_v)
       tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
+                  i0 + CH * (c - 1) + GT);
+    // the rounding residual of the same cells (16-bit stages 0 and 1)
+    if (with_r)
+      tma_load_3d(smem + (size_t)s * G::SLOT + G::R_OFF, &gd.tm_r, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
                   i0 + CH * (c - 1) + GT);
     if (c == nb) claim = atomicAdd(&queue[0], 1);  // the next tile's position, used one chunk later
     ps->c = c == nb ? 0 : c + 1;
@@ -679,38 +716,40 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
   if constexpr (Store<S>::DEV) {
 #pragma unroll
     for (int p = 0; p < NP; ++p) gr.bg[p] = make_float2(gd.dev.bg[2 * p], gd.dev.bg[2 * p + 1]);
-    gr.comp = lit<P>(a.comp_bg != 0.0 && dt > 0.0 ? 1.0 / (a.comp_bg * dt) : 0.0);
+    gr.comp = lit<P>(a.comp_bg != 0.0 && dt > 0.0 ? -1.0 / (a.comp_bg * dt) : 0.0);
     gr.scale = gd.dev.scale;
     gr.inv = gd.dev.inv;
+    gr.r = reinterpret_cast<S *>(gd.dev.r);
     gr.tiles2 = gd.dev.tiles2;
   }
 }
 
-// Deviation storage: decodes box columns c0 .. c0 + ncol of the landed 7-row u box (padded
-// rows prow0 .., box column 0 = padded column j0) into FP32 cells dec ([row][ncol][NV]):
-// bg + s h with s of the tile of the interior cell each value images.  This thread takes
-// every step-th column from `first`.
+// Deviation storage: decodes the landed 7-row u box (padded rows prow0 .., box column 0 =
+// padded column j0) into FP32 cells dec ([row][BOXW][NV]): bg + s h with s of the tile of the
+// interior cell each value images.  This thread takes every step-th column from `first`; the
+// scale-tile row of each of the 7 rows is found once per chunk.
 template <class S, int BOXW>
-__device__ __forceinline__ void decode_cols(const S *box, float *dec, int ncol, int c0, int first, int step, int prow0,
-                                            int j0, const GridRegs<S> &gr)
+__device__ __forceinline__ void decode_cols(const S *box, float *dec, int first, int step, int prow0, int j0,
+                                            const GridRegs<S> &gr)
 {
   const int n1 = gr.L.n1, n2 = gr.L.n2;
   const int i0 = prow0 - GT;
   const bool rows_inside = i0 >= 0 && i0 + CH <= n1;  // no ghost row in the box
-  for (int c = first; c < ncol; c += step) {
-    const int j = j0 - GL + c0 + c;
-    const int cc = c0 + c;
-    const int tj = (j >= 0 && j < n2 ? j : source_index(j, n2, gr.p2)) / SCALE_TILE;
+  int trow[CH];
+#pragma unroll
+  for (int r = 0; r < CH; ++r) trow[r] = ((rows_inside ? i0 + r : source_index(i0 + r, n1, gr.p1)) >> 6) * gr.tiles2;
+  for (int c = first; c < BOXW; c += step) {
+    const int j = j0 - GL + c;
+    const int tj = (j >= 0 && j < n2 ? j : source_index(j, n2, gr.p2)) >> 6;
 #pragma unroll
     for (int r = 0; r < CH; ++r) {
-      const int ti = (rows_inside ? i0 + r : source_index(i0 + r, n1, gr.p1)) / SCALE_TILE;
-      const float4 sc = __ldg(gr.scale + ti * gr.tiles2 + tj);
+      const float4 sc = __ldg(gr.scale + trow[r] + tj);
       const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
       float2 h[NP];
-      load_cell<S>(box + (r * BOXW + cc) * NV, h);
+      load_cell<S>(box + (r * BOXW + c) * NV, h);
 #pragma unroll
       for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
-      st_cell<float>(dec + (r * ncol + c) * NV, h);
+      st_cell<float>(dec + (r * BOXW + c) * NV, h);
     }
   }
 }
@@ -733,16 +772,106 @@ __device__ __forceinline__ void flush_grid(Status *st, bool &nan, T &rate)
   rate = T(0);
 }
 
+// Per-thread position in the launch: the current tile, its grid's registers and the block.
+template <class S>
+struct TileState {
+  using T = typename Store<S>::C;
+  GridRegs<S> gr;
+  int cur_g = -1;
+  int i0 = 0, j0 = 0, b = -1;      // tile origin and block (-1: the warm-up chunk)
+  int tj = 0;                      // scale-tile column of the thread's column (16-bit storage)
+  bool whole = false, rim = true;  // the tile lies inside the grid / within HALF cells of an edge
+  scheme::Geom<T> cg{};            // the scheme's geometry of the thread's column
+};
+
+// Enters launch tile `tile` of grid g (warp-uniform call: flushes the previous grid's NaN
+// flag and CFL max with warp collectives when the grid changes).
+template <class S, bool WRITE_U, bool CFL, bool SC, int W>
+__device__ __forceinline__ void enter_tile(TileState<S> &ts, const GridDesc *grids, int g, int tile,
+                                           const KParams<typename Store<S>::C> &a, bool &nan,
+                                           typename Store<S>::C &rate)
+{
+  using T = typename Store<S>::C;
+  if (g != ts.cur_g) {
+    if (ts.cur_g >= 0) flush_grid<WRITE_U, CFL>(ts.gr.status, nan, rate);
+    load_grid<S, SC>(grids[g], a, ts.gr);
+    ts.cur_g = g;
+  }
+  const int local = tile - grids[g].tile0, strips = grids[g].strips;
+  const int th = a.nb * CH;
+  ts.i0 = (local / strips) * th;
+  ts.j0 = (local % strips) * W;
+  ts.b = -1;
+  const int j = ts.j0 + (int)threadIdx.x;
+  ts.whole = ts.i0 + th <= ts.gr.L.n1 && ts.j0 + W <= ts.gr.L.n2;
+  ts.cg = scheme::column_geom<T>(j, SC ? ts.gr.delta2 : a.ks.delta2);
+  ts.rim = ts.i0 < HALF || ts.i0 + th > ts.gr.L.n1 - HALF || ts.j0 < HALF || ts.j0 + W > ts.gr.L.n2 - HALF;
+  if constexpr (Store<S>::DEV) ts.tj = min(j, ts.gr.L.n2 - 1) >> 6;
+}
+
+// The stencil work of one chunk: the warm-up chunk's 7 rows only feed the window and the
+// accumulators; a block's 7 leading rows each complete the output row 3 behind.  base points
+// at column j - 3 of the chunk's row 0 (the landed box, or its decoded copy); sbox is the
+// chunk's slot (v and r boxes).
+template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC, int W>
+__device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, const S *sbox, TileState<S> &ts,
+                                              const KParams<typename Store<S>::C> &a,
+                                              Roll<typename Store<S>::C> &st, bool &nan, typename Store<S>::C &rate)
+{
+  using T = typename Store<S>::C;
+  using P = typename PairOf<T>::type;
+  constexpr bool RR = Store<S>::DEV && WRITE_U && WRITE_V;
+  using G = Geo<S, READ_V, RR, W>;
+  constexpr int BW = Strip<W>::BW;
+  const int tx = threadIdx.x;
+  if (ts.b < 0) {
+#pragma unroll
+    for (int g2 = 0; g2 < ND12; ++g2)
+#pragma unroll
+      for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
+    lead_row<T, M2, 0, BW * NV>(base, a, st);
+    lead_row<T, M2, 1, BW * NV>(base, a, st);
+    lead_row<T, M2, 2, BW * NV>(base, a, st);
+    lead_row<T, M2, 3, BW * NV>(base, a, st);
+    lead_row<T, M2, 4, BW * NV>(base, a, st);
+    lead_row<T, M2, 5, BW * NV>(base, a, st);
+    lead_row<T, M2, 6, BW * NV>(base, a, st);
+  } else {
+    const int ib = ts.i0 + CH * ts.b, j = ts.j0 + tx;
+    const S *sv = sbox + G::V_OFF / sizeof(S);
+    const S *sr = sbox + G::R_OFF / sizeof(S);
+#define FG2_ROW(R)                                                                                         \
+  {                                                                                                        \
+    P vrow[NP], rrow[NP];                                                                                  \
+    if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                                 \
+    if (RR) load_cell<S>(sr + (R * G::VBW + tx + G::VOFF) * NV, rrow);                                     \
+    lead_row<T, M2, R, BW * NV>(base, a, st);                                                              \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, ts.tj, a, ts.gr, st, ts.whole, \
+                                                          ts.rim, nan, rate, ts.cg);                       \
+  }
+    FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
+#undef FG2_ROW
+  }
+}
+
+// Chunk loop.  Every thread waits (bounded) for its chunk itself; the one CTA barrier per
+// chunk both agrees on a timeout (__syncthreads_or) and hands the consumed slot back to the
+// issuing thread.  A thread whose wait ran out skips the chunk's work (its bookkeeping is
+// not yet visible to it), and the CTA leaves together at that barrier.
+//   FP32 / FP64 storage: wait for chunk n, stencil it from its slot, barrier, refill the slot.
+//   16-bit storage: chunk n was decoded into dec[n & 1] during the previous chunk; stencil it,
+//   wait for chunk n + 1 and decode it into the other copy, barrier, refill chunk n's slot.
 template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC, int W>
 __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4 ? 2 : 3) * (128 / W) : 128 / W) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
                                                          const KParams<typename Store<S>::C> a, int *queue)
 {
   using T = typename Store<S>::C;
-  using P = typename PairOf<T>::type;
-  using G = Geo<S, READ_V, W>;
-  constexpr int SW = Strip<W>::SW, BW = Strip<W>::BW, NT = Strip<W>::NT;
   constexpr bool DEV = Store<S>::DEV;
+  constexpr bool RR = DEV && WRITE_U && WRITE_V;  // the stage reads the rounding residual
+  using G = Geo<S, READ_V, RR, W>;
+  constexpr int BW = Strip<W>::BW, NT = Strip<W>::NT;
   constexpr int NS = G::NSLOT;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
   int *tile_of = reinterpret_cast<int *>(full + NS);
@@ -759,94 +888,85 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
     ps->c = 0;
     ps->done = 0;
     claim = atomicAdd(&queue[0], 1);
-    for (int s = 0; s < NS; ++s) issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue, claim);
+    for (int s = 0; s < NS; ++s)
+      issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+                                    a.wait_test_bytes, queue, claim);
   }
   __syncthreads();
 
   bool nan = false;
   T rate = T(0);
   const int tx = threadIdx.x;  // column within the strip
-  GridRegs<S> gr;
-  int cur_g = -1;
+  TileState<S> ts;
   Roll<T> st;
-  int n = 0;  // chunks consumed
-  int i0 = 0, j0 = 0, b = -1;  // current tile and block (-1: warm-up chunk)
-  bool whole = false, rim = true;  // the tile lies inside the grid / within HALF cells of an edge
-  scheme::Geom<T> cg{};            // the scheme's geometry of this thread's column (per tile)
-  // the stencil's source: the landed box, or (16-bit storage) its decoded copy
   float *dec = reinterpret_cast<float *>(smem + G::DEC_OFF);
-
-  for (;;) {
+  auto slot = [&](int n) { return reinterpret_cast<const S *>(smem + (size_t)(n % NS) * G::SLOT); };
+  auto parity = [&](int n) { return (uint32_t)((n / NS) & 1); };
+  // padded row of the u box's row 0 for the thread's current tile and block
+  auto box_row = [&]() { return ts.b < 0 ? ts.i0 - 4 + GT : ts.i0 + CH * ts.b + 3 + GT; };
+  // the tile state for chunk n: a new tile after the last block of the previous one (tile < 0:
+  // the end of the queue); returns false at the end
+  auto advance = [&](int n) {
+    if (ts.cur_g >= 0 && ts.b < a.nb - 1) {  // the next block of the current tile
+      ++ts.b;
+      return true;
+    }
     const int s = n % NS;
-    const uint32_t parity = (uint32_t)((n / NS) & 1);
-    // the chunk has landed (every thread waits, the CTA agrees)
-    const bool landed = mbar_wait_bounded(&full[s], parity, WAIT_NS);
-    if (__syncthreads_or(!landed)) {
-      if (threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
-      break;
-    }
-    const S *sbox = reinterpret_cast<const S *>(smem + (size_t)s * G::SLOT);
-    // column j - 3 of the box's row 0
-    const T *base = (DEV ? reinterpret_cast<const T *>(dec) : reinterpret_cast<const T *>(sbox)) + (tx + GL - 3) * NV;
-    int prow0;  // padded row of the box's first row
-    if (b < 0) {
-      const int tile = tile_of[s];
-      if (tile < 0) break;
-      const int g = grid_of[s];
-      if (g != cur_g) {
-        if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);
-        load_grid<S, SC>(grids[g], a, gr);
-        cur_g = g;
-      }
-      const int local = tile - grids[g].tile0, strips = grids[g].strips;
-      i0 = (local / strips) * (a.nb * CH);
-      j0 = (local % strips) * SW;
-      prow0 = i0 - 4 + GT;
-      const int th = a.nb * CH;
-      whole = i0 + th <= gr.L.n1 && j0 + SW <= gr.L.n2;
-      cg = scheme::column_geom<T>(j0 + tx, SC ? gr.delta2 : a.ks.delta2);
-      rim = i0 < HALF || i0 + th > gr.L.n1 - HALF || j0 < HALF || j0 + SW > gr.L.n2 - HALF;
-    } else {
-      prow0 = i0 + CH * b + 3 + GT;
-    }
-    if constexpr (DEV) {
-      decode_cols<S, BW>(sbox, dec, BW, 0, tx, NT, prow0, j0, gr);
-      __syncthreads();
-    }
-    if (b < 0) {
-#pragma unroll
-      for (int g2 = 0; g2 < ND12; ++g2)
-#pragma unroll
-        for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
-      // warm-up chunk: rows i0-4 .. i0+2 only feed the window and the accumulators
-      lead_row<T, M2, 0, BW * NV>(base, a, st);
-      lead_row<T, M2, 1, BW * NV>(base, a, st);
-      lead_row<T, M2, 2, BW * NV>(base, a, st);
-      lead_row<T, M2, 3, BW * NV>(base, a, st);
-      lead_row<T, M2, 4, BW * NV>(base, a, st);
-      lead_row<T, M2, 5, BW * NV>(base, a, st);
-      lead_row<T, M2, 6, BW * NV>(base, a, st);
-    } else {
-      const int ib = i0 + CH * b, j = j0 + tx;
-      const S *sv = sbox + G::V_OFF / sizeof(S);
-#define FG2_ROW(R)                                                                                \
-  {                                                                                               \
-    P vrow[NP];                                                                                   \
-    if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                        \
-    lead_row<T, M2, R, BW * NV>(base, a, st);                                                     \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, a, gr, st, whole, rim, nan, rate, cg); \
-  }
-      FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
-#undef FG2_ROW
-    }
-    __syncthreads();  // everyone is done with slot s
-    if (threadIdx.x == 0)
-      issue_chunk<S, READ_V, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0, a.wait_test_bytes, queue, claim);  // refill slot s
-    ++n;
-    b = b == a.nb - 1 ? -1 : b + 1;
-  }
+    const int tile = tile_of[s];
+    if (tile < 0) return false;
+    enter_tile<S, WRITE_U, CFL, SC, W>(ts, grids, grid_of[s], tile, a, nan, rate);
+    return true;
+  };
+  bool failed = false;
 
-  if (cur_g >= 0) flush_grid<WRITE_U, CFL>(gr.status, nan, rate);
+  if constexpr (!DEV) {
+    for (int n = 0;; ++n) {
+      const bool landed = mbar_wait_bounded(&full[n % NS], parity(n), WAIT_NS);
+      bool live = false;
+      if (__all_sync(FULL, landed)) {
+        live = advance(n);
+        if (live)
+          stencil_chunk<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC, W>(reinterpret_cast<const T *>(slot(n)) + (tx + GL - 3) * NV,
+                                                                     slot(n), ts, a, st, nan, rate);
+      }
+      if (__syncthreads_or(!landed)) {
+        failed = true;
+        break;
+      }
+      if (!live) break;  // the end of the queue (the same chunk for every thread)
+      if (threadIdx.x == 0)
+        issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+                                      a.wait_test_bytes, queue, claim);  // refill chunk n's slot
+    }
+  } else {
+    // chunk 0: wait, decode
+    bool landed = mbar_wait_bounded(&full[0], parity(0), WAIT_NS);
+    bool live = false;
+    if (__all_sync(FULL, landed)) {
+      live = advance(0);
+      if (live) decode_cols<S, BW>(slot(0), dec, tx, NT, box_row(), ts.j0, ts.gr);
+    }
+    failed = __syncthreads_or(!landed);
+    for (int n = 0; live && !failed; ++n) {
+      stencil_chunk<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC, W>(
+          dec + (size_t)(n & 1) * (G::DEC_ONE / sizeof(float)) + (tx + GL - 3) * NV, slot(n), ts, a, st, nan, rate);
+      landed = mbar_wait_bounded(&full[(n + 1) % NS], parity(n + 1), WAIT_NS);
+      live = false;
+      if (__all_sync(FULL, landed)) {
+        live = advance(n + 1);
+        if (live)
+          decode_cols<S, BW>(slot(n + 1), dec + (size_t)((n + 1) & 1) * (G::DEC_ONE / sizeof(float)), tx, NT, box_row(),
+                             ts.j0, ts.gr);
+      }
+      failed = __syncthreads_or(!landed);
+      if (!failed && live && threadIdx.x == 0)
+        issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+                                      a.wait_test_bytes, queue, claim);  // refill chunk n's slot
+    }
+  }
+  if (failed && threadIdx.x == 0) atomicOr(&a.status->error, ERR_TMA_TIMEOUT);
+
+  if (ts.cur_g >= 0) flush_grid<WRITE_U, CFL>(ts.gr.status, nan, rate);
 
   __syncthreads();
   if (threadIdx.x == 0) {

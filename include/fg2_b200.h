@@ -81,6 +81,16 @@ int fg2_sim_set_bcond(fg2_sim *s, int p1, int p2);
  * the reference (its block shape came from setup()'s heuristic, src/setup.cpp:39-58); results
  * are bitwise the same for every height. */
 int fg2_sim_set_tiling(fg2_sim *s, int nb);
+/* CTAs per SM of the fused kernel's persistent grid (0: as many as fit), and the current
+ * tiling (the tile height the launches use, after the default's small-grid rule). */
+int fg2_sim_set_occupancy(fg2_sim *s, int ctas_per_sm);
+int fg2_sim_get_tiling(const fg2_sim *s, int *nb, int *ctas_per_sm);
+/* Times reps steps of each tiling candidate (tile height 1..8 blocks x occupancy cap: all
+ * that fit, 4, 8 or 12 warps per SM) on the simulation's own state with dt = 0 (the state
+ * is left bitwise unchanged; 16-bit storage is kept aside and put back) and keeps the
+ * fastest; best_ms (may be NULL) receives its time per step.  The successor, for one grid,
+ * of the reference's block-size heuristic (src/setup.cpp:39-58). */
+int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms);
 /* para() (src/para.cpp:25-40): "key=val" (leading dashes skipped); returns "key = val" in a
  * buffer owned by the handle, or NULL for an unknown key. */
 const char *fg2_sim_para(fg2_sim *s, const char *keyval);

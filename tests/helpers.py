@@ -42,3 +42,58 @@ def rel_l2(a, b):
     num = np.sqrt(((a - b) ** 2).sum(0))
     den = np.sqrt((b ** 2).sum(0))
     return num / np.where(den > 0, den, 1.0)
+
+
+# ---- 16-bit deviation storage, emulated on the CPU ----------------------------------------
+SCALE_TILE = 64
+
+
+def round_bf16(a):
+    """Round to the nearest BF16 number (ties to even), returned as float64."""
+    b = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def round16(a, storage):
+    return np.asarray(a, np.float16).astype(np.float64) if storage == "f16" else round_bf16(a)
+
+
+def deviation_codes(x0, reflect=(2,)):
+    """The storage's codes for the initial state x0 (n1, n2, NVAR): per-field background (the
+    field mean; 0 for the fields a reflecting wall negates) and per-64x64-tile scale (the largest
+    deviation on the tile, 1 where there is none), broadcast to cells."""
+    n1, n2, nv = x0.shape
+    bg = x0.reshape(-1, nv).mean(0)
+    for f in reflect:
+        bg[f] = 0.0
+    t1, t2 = -(-n1 // SCALE_TILE), -(-n2 // SCALE_TILE)
+    pad = np.full((t1 * SCALE_TILE, t2 * SCALE_TILE, nv), np.nan)
+    pad[:n1, :n2] = np.abs(x0 - bg)
+    s = np.nanmax(pad.reshape(t1, SCALE_TILE, t2, SCALE_TILE, nv), axis=(1, 3))
+    # a field equal to its background on a tile (to the float rounding of the mean) has scale 1
+    s[~(s > 1e-6 * np.maximum(np.abs(bg), 1.0))] = 1.0
+    return bg, np.repeat(np.repeat(s, SCALE_TILE, 0), SCALE_TILE, 1)[:n1, :n2]
+
+
+def stencil_on_codes(oracle, x0, steps, dt, storage, p1=1, p2=1):
+    """The accuracy floor of any scheme whose stencil reads the 16-bit numbers: the state T is
+    kept exactly (FP64, every rounding compensated), but each substage evaluates the right-hand
+    side on the numbers the storage holds for T, bg + s round16((T - bg) / s).  `oracle` is
+    an FP64 Oracle with its Delta set.  Returns T after `steps` RK3 steps."""
+    from oracle.oracle import HALO
+    beta = [0.0, -5.0 / 9.0, -153.0 / 128.0]
+    gamma = [1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0]
+    bg, s = deviation_codes(x0)
+    T = np.asarray(x0, np.float64).copy()
+    n1, n2, _ = T.shape
+    up = oracle.padded(T)
+    vp = oracle.padded(np.zeros_like(T))
+    inner = (slice(HALO, HALO + n1), slice(HALO, HALO + n2))
+    for _ in range(steps):
+        for k in range(3):
+            up[inner] = bg + s * round16((T - bg) / s, storage)
+            oracle.bcond(up, p1, p2)
+            oracle.kick(vp, up, 0.0, beta[k])
+            T = T + gamma[k] * dt * vp[inner]
+    return T

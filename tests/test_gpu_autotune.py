@@ -1,0 +1,38 @@
+"""The single-grid autotuner (fg2_sim_autotune), the successor for one grid of the reference's
+block-size heuristic (src/setup.cpp:39-58): it times steps of dt = 0 on the simulation's own
+state for every tile height x occupancy candidate and keeps the fastest.  The state must come
+out bitwise unchanged (FP32, and 16-bit storage with its rounding residual), and the chosen
+tiling must give bitwise the results of the default one."""
+import numpy as np
+import pytest
+
+import fg2_b200
+
+pytestmark = pytest.mark.gpu
+
+
+def steps(s, nsteps, dt):
+    t = 0.0
+    for _ in range(nsteps):
+        assert s.step(t, dt) == 0
+        t += dt
+    return s.download()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("n1,n2", [(300, 260), (1024, 1024)])
+def test_autotune_leaves_the_state_and_the_results_unchanged(storage, n1, n2, cuda):
+    x = fg2_b200.setup_evaluate("kh", n1, n2, seed=9)[0].astype(np.float32)
+    dt = 2e-5
+    with fg2_b200.Sim(n1, n2, storage=storage) as a, fg2_b200.Sim(n1, n2, storage=storage) as b:
+        for s in (a, b):
+            s.config()
+            s.upload(x)
+        before = a.download()
+        ms = a.autotune(reps=2)
+        assert ms > 0
+        nb, ctas = a.tiling()
+        assert 1 <= nb <= 8 and ctas >= 0
+        assert np.array_equal(a.download(), before)
+        # the tuned tiling and the default one give bitwise the same steps
+        assert np.array_equal(steps(a, 3, dt), steps(b, 3, dt))

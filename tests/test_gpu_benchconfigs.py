@@ -10,7 +10,10 @@
   64-member hydro batch (sides 512..2048), each advanced as one batch; members of the largest
   and smallest sides are compared with the port stepping them alone.
 
-Bar: per-field relative L2 <= 1e-5 (FP32 against FP32 arithmetic, the documented bar)."""
+Bar: per-field relative L2 <= 1e-5 (FP32 against FP32 arithmetic, the documented bar).  The
+turbulent batch members start from ln rho = 0 with a divergence-free velocity, so after a few
+steps ln rho is a tiny field of its own rounding size; their first field is compared as the
+density rho = exp(ln rho) instead."""
 import os
 import sys
 
@@ -82,10 +85,16 @@ def batch_members_against_the_port(scheme, sizes, seed_of, box, dt, nsteps, setu
         assert b.advance(nsteps, dt, graph=True) == 0
         assert b.sync() == 0
         out = {k: b.members[k].download() for k in sample}
+
+    def density_first(x):
+        y = x.astype(np.float64)
+        y[..., 0] = np.exp(y[..., 0])
+        return y
+
     for k in sample:
         n1, n2 = sizes[k]
         ref = cpu_steps(oracle(scheme, n1, n2, *box, prefer="port"), x0[k], nsteps, dt)
-        err = rel_l2(out[k], ref)
+        err = rel_l2(density_first(out[k]), density_first(ref))
         assert np.all(err <= 1e-5), (k, sizes[k], err)
 
 
