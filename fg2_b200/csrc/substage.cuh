@@ -479,10 +479,18 @@ __device__ __noinline__ void rim_images3(S *u, const Layout L, int i, int j, typ
 
 // The same for 16-bit storage, with the stored numbers (reflected fields have bg = 0, so their
 // images are the negated numbers).
+// The stored numbers of one cell, passed by value (an array argument would put every cell's
+// numbers through local memory, rim or not).
 template <class S>
-__device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, const S *raw, int p1, int p2)
+struct RawCell {
+  S v[NV];
+};
+
+template <class S>
+__device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, const RawCell<S> rc, int p1, int p2)
 {
   const int n1 = L.n1, n2 = L.n2;
+  const S *raw = rc.v;
   if (n1 < 2 * HALF || n2 < 2 * HALF) {
     store_ghosts<S, S>(u, L, i, j, raw, p1, p2);
     return;
@@ -516,7 +524,8 @@ __device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, 
 // 2 reads once, with no carry beyond it.  The stencil itself reads S.
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP],
-                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j, int tj,
+                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j,
+                                         const float4 &scv, const float4 &ivv,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
                                          const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
                                          typename Store<S>::C &rate, const scheme::Geom<typename Store<S>::C> &cg)
@@ -543,13 +552,11 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
   P sc[NP], iv[NP];  // deviation storage: the scales of the cell's tile
   if constexpr (DEV && WRITE_U) {
-    const int t = (i >> 6) * gr.tiles2 + tj;  // SCALE_TILE = 64
-    const float4 x = __ldg(gr.scale + t), y = __ldg(gr.inv + t);
-    sc[0] = make_float2(x.x, x.y);
-    iv[0] = make_float2(y.x, y.y);
+    sc[0] = make_float2(scv.x, scv.y);
+    iv[0] = make_float2(ivv.x, ivv.y);
     if constexpr (NP > 1) {
-      sc[NP - 1] = make_float2(x.z, x.w);
-      iv[NP - 1] = make_float2(y.z, y.w);
+      sc[NP - 1] = make_float2(scv.z, scv.w);
+      iv[NP - 1] = make_float2(ivv.z, ivv.w);
     }
   }
   P vn[NP], qp[NP];
@@ -566,14 +573,14 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
     if (WRITE_U) store_cell<S>(gr.u_out + o, qp);
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
-  S raw[NV];
+  RawCell<S> raw;
   if constexpr (DEV) {
     if (WRITE_U) {
       // encode u' with its tile's 1/s; e' = S' - u' is the rounding residual
       P h[NP], hs[NP], e[NP];
 #pragma unroll
       for (int p = 0; p < NP; ++p) h[p] = (qp[p] - gr.bg[p]) * iv[p];
-      encode_cell<S>(gr.u_out + o, h, hs, raw);
+      encode_cell<S>(gr.u_out + o, h, hs, raw.v);
 #pragma unroll
       for (int p = 0; p < NP; ++p) e[p] = fmac(sc[p], hs[p], gr.bg[p]) - qp[p];
       if constexpr (FOLD) {
@@ -726,31 +733,44 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
 
 // Deviation storage: decodes the landed 7-row u box (padded rows prow0 .., box column 0 =
 // padded column j0) into FP32 cells dec ([row][BOXW][NV]): bg + s h with s of the tile of the
-// interior cell each value images.  This thread takes every step-th column from `first`; the
-// scale-tile row of each of the 7 rows is found once per chunk.
-template <class S, int BOXW>
-__device__ __forceinline__ void decode_cols(const S *box, float *dec, int first, int step, int prow0, int j0,
-                                            const GridRegs<S> &gr)
+// interior cell each value images.  Thread t decodes column t of every row and, for t below
+// 7 (BOXW - NT), one cell of the columns beyond the strip, so the work is even across warps.
+// A chunk whose 7 rows lie in one tile row (all but about one chunk in nine) reads each
+// column's scales once.
+template <class S, int BOXW, int NT>
+__device__ __forceinline__ void decode_box(const S *box, float *dec, int tx, int prow0, int j0, const GridRegs<S> &gr)
 {
+  constexpr int EXTRA = BOXW - NT;  // columns beyond one per thread
   const int n1 = gr.L.n1, n2 = gr.L.n2;
   const int i0 = prow0 - GT;
   const bool rows_inside = i0 >= 0 && i0 + CH <= n1;  // no ghost row in the box
-  int trow[CH];
-#pragma unroll
-  for (int r = 0; r < CH; ++r) trow[r] = ((rows_inside ? i0 + r : source_index(i0 + r, n1, gr.p1)) >> 6) * gr.tiles2;
-  for (int c = first; c < BOXW; c += step) {
+  auto row_tile = [&](int r) { return ((rows_inside ? i0 + r : source_index(i0 + r, n1, gr.p1)) >> 6) * gr.tiles2; };
+  auto col_tile = [&](int c) {
     const int j = j0 - GL + c;
-    const int tj = (j >= 0 && j < n2 ? j : source_index(j, n2, gr.p2)) >> 6;
+    return (j >= 0 && j < n2 ? j : source_index(j, n2, gr.p2)) >> 6;
+  };
+  auto put = [&](int r, int c, float4 sc) {
+    const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
+    float2 h[NP];
+    load_cell<S>(box + (r * BOXW + c) * NV, h);
 #pragma unroll
-    for (int r = 0; r < CH; ++r) {
-      const float4 sc = __ldg(gr.scale + trow[r] + tj);
-      const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
-      float2 h[NP];
-      load_cell<S>(box + (r * BOXW + c) * NV, h);
+    for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
+    st_cell<float>(dec + (r * BOXW + c) * NV, h);
+  };
+  {
+    const int tj = col_tile(tx);
+    if (rows_inside && (i0 >> 6) == ((i0 + CH - 1) >> 6)) {
+      const float4 sc = __ldg(gr.scale + (i0 >> 6) * gr.tiles2 + tj);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
-      st_cell<float>(dec + (r * BOXW + c) * NV, h);
+      for (int r = 0; r < CH; ++r) put(r, tx, sc);
+    } else {
+#pragma unroll
+      for (int r = 0; r < CH; ++r) put(r, tx, __ldg(gr.scale + row_tile(r) + tj));
     }
+  }
+  if (tx < CH * EXTRA) {  // the EXTRA columns right of the strip, one cell per thread
+    const int r = tx / EXTRA, c = NT + tx % EXTRA;
+    put(r, c, __ldg(gr.scale + row_tile(r) + col_tile(c)));
   }
 }
 
@@ -840,14 +860,28 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
     const int ib = ts.i0 + CH * ts.b, j = ts.j0 + tx;
     const S *sv = sbox + G::V_OFF / sizeof(S);
     const S *sr = sbox + G::R_OFF / sizeof(S);
+    // 16-bit storage: the scales of the output rows' tile, loaded once per chunk and again at
+    // the row where the chunk crosses into the next tile row (CTA-uniform)
+    float4 scv = make_float4(0.f, 0.f, 0.f, 0.f), ivv = scv;
+    int next_tile_row = 1 << 30;
+    if constexpr (Store<S>::DEV && WRITE_U) {
+      const int r0 = min(ib, ts.gr.L.n1 - 1) >> 6;
+      scv = __ldg(ts.gr.scale + r0 * ts.gr.tiles2 + ts.tj);
+      ivv = __ldg(ts.gr.inv + r0 * ts.gr.tiles2 + ts.tj);
+      if (((r0 + 1) << 6) < ts.gr.L.n1) next_tile_row = (r0 + 1) << 6;
+    }
 #define FG2_ROW(R)                                                                                         \
   {                                                                                                        \
     P vrow[NP], rrow[NP];                                                                                  \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                                 \
     if (RR) load_cell<S>(sr + (R * G::VBW + tx + G::VOFF) * NV, rrow);                                     \
+    if (Store<S>::DEV && WRITE_U && ib + R == next_tile_row) {                                             \
+      scv = __ldg(ts.gr.scale + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);                              \
+      ivv = __ldg(ts.gr.inv + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);                                \
+    }                                                                                                      \
     lead_row<T, M2, R, BW * NV>(base, a, st);                                                              \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, ts.tj, a, ts.gr, st, ts.whole, \
-                                                          ts.rim, nan, rate, ts.cg);                       \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, scv, ivv, a, ts.gr, st,    \
+                                                          ts.whole, ts.rim, nan, rate, ts.cg);             \
   }
     FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
@@ -944,7 +978,7 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
     bool live = false;
     if (__all_sync(FULL, landed)) {
       live = advance(0);
-      if (live) decode_cols<S, BW>(slot(0), dec, tx, NT, box_row(), ts.j0, ts.gr);
+      if (live) decode_box<S, BW, NT>(slot(0), dec, tx, box_row(), ts.j0, ts.gr);
     }
     failed = __syncthreads_or(!landed);
     for (int n = 0; live && !failed; ++n) {
@@ -955,8 +989,8 @@ __global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4
       if (__all_sync(FULL, landed)) {
         live = advance(n + 1);
         if (live)
-          decode_cols<S, BW>(slot(n + 1), dec + (size_t)((n + 1) & 1) * (G::DEC_ONE / sizeof(float)), tx, NT, box_row(),
-                             ts.j0, ts.gr);
+          decode_box<S, BW, NT>(slot(n + 1), dec + (size_t)((n + 1) & 1) * (G::DEC_ONE / sizeof(float)), tx, box_row(),
+                                ts.j0, ts.gr);
       }
       failed = __syncthreads_or(!landed);
       if (!failed && live && threadIdx.x == 0)

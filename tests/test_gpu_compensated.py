@@ -59,7 +59,7 @@ def test_upload_keeps_the_residual(storage, cuda):
     assert np.all(err <= RESID[storage] * scale + 4 * np.spacing(np.abs(x).astype(np.float32))), err.max()
 
 
-@pytest.mark.parametrize("storage,dt", [("f16", 1e-5), ("bf16", 8e-5)])
+@pytest.mark.parametrize("storage,dt", [("f16", 4e-6), ("bf16", 3.2e-5)])
 def test_increments_below_half_a_unit_accumulate(storage, dt, cuda):
     """Grid-scale velocity noise (sigma 0.01) decays by viscosity at about a fifth of a 16-bit
     unit (of the tile scale) per step at this dt; over 20 steps the FP32 state moves by
