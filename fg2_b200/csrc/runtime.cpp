@@ -593,9 +593,16 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
     c.ms = ms / (2.0 * reps);
     return FG2_OK;
   };
-  int rc = FG2_OK;
-  for (size_t i = 0; i < cands.size() && rc == 0; ++i) rc = measure(cands[i]);
-  if (rc == 0) {  // the three best again, each scored by its faster measurement
+  // the default tiling first: a step shorter than LAUNCH_BOUND_MS is bound by launch latency,
+  // which no tiling changes and which hides the kernel's own time, so such grids keep the
+  // default (its small-grid rule gives every resident CTA a tile)
+  constexpr double LAUNCH_BOUND_MS = 0.05;
+  Cand dflt{0, 0, 0.0};
+  int rc = measure(dflt);
+  const bool launch_bound = rc == 0 && dflt.ms < LAUNCH_BOUND_MS;
+  if (launch_bound) cands.assign(1, dflt);
+  for (size_t i = 0; i < cands.size() && rc == 0 && !launch_bound; ++i) rc = measure(cands[i]);
+  if (rc == 0 && !launch_bound) {  // the three best again, each scored by its faster measurement
     std::sort(cands.begin(), cands.end(), [](const Cand &x, const Cand &y) { return x.ms < y.ms; });
     for (size_t i = 0; i < 3 && i < cands.size() && rc == 0; ++i) {
       const double first = cands[i].ms;

@@ -888,6 +888,17 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
   }
 }
 
+// Resident CTAs per SM the register budget is cut for (128-column strips; twice that for 64):
+// 4 for three-field FP32 cells (at most 128 registers, no spills), 3 for four fields and for
+// 16-bit storage, 2 for six-field FP32 cells; FP64 kernels are not bounded below one.
+template <class S, int W>
+__host__ __device__ constexpr int min_blocks()
+{
+  return sizeof(typename Store<S>::C) != 4 ? 128 / W
+         : Store<S>::DEV                    ? 3 * (128 / W)
+                                            : (NV > 4 ? 2 : NV == 3 ? 4 : 3) * (128 / W);
+}
+
 // Chunk loop.  Every thread waits (bounded) for its chunk itself; the one CTA barrier per
 // chunk both agrees on a timeout (__syncthreads_or) and hands the consumed slot back to the
 // issuing thread.  A thread whose wait ran out skips the chunk's work (its bookkeeping is
@@ -896,7 +907,7 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
 //   16-bit storage: chunk n was decoded into dec[n & 1] during the previous chunk; stencil it,
 //   wait for chunk n + 1 and decode it into the other copy, barrier, refill chunk n's slot.
 template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC, int W>
-__global__ void __launch_bounds__(W, sizeof(typename Store<S>::C) == 4 ? (NV > 4 ? 2 : 3) * (128 / W) : 128 / W) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
+__global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const GridDesc *__restrict__ grids, int ngrids, int ntiles,
                                                          const KParams<typename Store<S>::C> a, int *queue)
 {
   using T = typename Store<S>::C;

@@ -88,8 +88,9 @@ int fg2_sim_get_tiling(const fg2_sim *s, int *nb, int *ctas_per_sm);
 /* Times reps steps of each tiling candidate (tile height 1..8 blocks x occupancy cap: all
  * that fit, 4, 8 or 12 warps per SM) on the simulation's own state with dt = 0 (the state
  * is left bitwise unchanged; 16-bit storage is kept aside and put back) and keeps the
- * fastest; best_ms (may be NULL) receives its time per step.  The successor, for one grid,
- * of the reference's block-size heuristic (src/setup.cpp:39-58). */
+ * fastest; best_ms (may be NULL) receives its time per step.  A grid whose step takes under
+ * 0.05 ms with the default tiling is bound by launch latency and keeps the default.  The
+ * successor, for one grid, of the reference's block-size heuristic (src/setup.cpp:39-58). */
 int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms);
 /* para() (src/para.cpp:25-40): "key=val" (leading dashes skipped); returns "key = val" in a
  * buffer owned by the handle, or NULL for an unknown key. */
