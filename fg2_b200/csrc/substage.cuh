@@ -298,7 +298,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 
 // Leading-row work of field pair PI for register slot R, from the pair's values at
 // columns j-3 .. j+3 of the leading row.
-template <class T, unsigned M2, int R, int PI>
+// D2: the row is an output row of the tile, so its axis-2 derivatives are needed (the warm-up
+// rows above the tile only feed the window and the mixed-derivative accumulators).
+template <class T, unsigned M2, int R, int PI, bool D2>
 __device__ __forceinline__ void lead_pair(const typename PairOf<T>::type (&x)[7][NP], const KParams<T> &a, Roll<T> &s,
                                           typename PairOf<T>::type dk[3])
 {
@@ -308,6 +310,7 @@ __device__ __forceinline__ void lead_pair(const typename PairOf<T>::type (&x)[7]
   dk[0] = r1 - l1;
   dk[1] = r2 - l2;
   dk[2] = r3 - l3;
+  if constexpr (!D2) return;
   s.h2[PI][R] = fmac(a.k.a2[0], dk[0], fmac(a.k.a2[1], dk[1], a.k.a2[2] * dk[2]));
   constexpr bool nx = need<M2>(2 * PI), ny = need<M2>(2 * PI + 1);
   if constexpr (nx && ny) {
@@ -356,7 +359,7 @@ __device__ __forceinline__ void d12_emit(const GR &gr, const Roll<T> &s, Cell<T,
 
 // Leading-row work for register slot R: loads the 7 cells of row R of the chunk around the
 // thread's column; base points at column j-3 of row 0, rows are RSTRIDE elements apart.
-template <class T, unsigned M2, int R, int RSTRIDE>
+template <class T, unsigned M2, int R, int RSTRIDE, bool D2 = true>
 __device__ __forceinline__ void lead_row(const T *base, const KParams<T> &a, Roll<T> &s)
 {
   using P = typename PairOf<T>::type;
@@ -365,9 +368,9 @@ __device__ __forceinline__ void lead_row(const T *base, const KParams<T> &a, Rol
 #pragma unroll
   for (int k = 0; k < 7; ++k) ld_cell<T>(row + k * NV, x[k]);
   P dk[NP][3];
-  lead_pair<T, M2, R, 0>(x, a, s, dk[0]);
-  if constexpr (NP > 1) lead_pair<T, M2, R, 1>(x, a, s, dk[1]);
-  if constexpr (NP > 2) lead_pair<T, M2, R, 2>(x, a, s, dk[2]);
+  lead_pair<T, M2, R, 0, D2>(x, a, s, dk[0]);
+  if constexpr (NP > 1) lead_pair<T, M2, R, 1, D2>(x, a, s, dk[1]);
+  if constexpr (NP > 2) lead_pair<T, M2, R, 2, D2>(x, a, s, dk[2]);
   d12_lead<T, R, 0>(dk, a, s);
 }
 
@@ -849,10 +852,11 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
     for (int g2 = 0; g2 < ND12; ++g2)
 #pragma unroll
       for (int q = 0; q < CH; ++q) st.x[g2][q] = T(0);
-    lead_row<T, M2, 0, BW * NV>(base, a, st);
-    lead_row<T, M2, 1, BW * NV>(base, a, st);
-    lead_row<T, M2, 2, BW * NV>(base, a, st);
-    lead_row<T, M2, 3, BW * NV>(base, a, st);
+    // row i0 - 4 (box row 0) feeds no output row of the tile; rows i0 - 3 .. i0 - 1 feed the
+    // window and the mixed derivatives only; rows i0 .. i0 + 2 are output rows
+    lead_row<T, M2, 1, BW * NV, false>(base, a, st);
+    lead_row<T, M2, 2, BW * NV, false>(base, a, st);
+    lead_row<T, M2, 3, BW * NV, false>(base, a, st);
     lead_row<T, M2, 4, BW * NV>(base, a, st);
     lead_row<T, M2, 5, BW * NV>(base, a, st);
     lead_row<T, M2, 6, BW * NV>(base, a, st);
