@@ -171,6 +171,28 @@ def test_autotune_keeps_state(cuda):
         close(b, alone)
 
 
+def test_autotune_keeps_16_bit_members_and_their_residuals(cuda):
+    """A step of dt = 0 re-encodes 16-bit members and drops their rounding residuals, so the
+    tuner keeps the members' arrays aside: the compensated states come back bitwise, and the
+    next steps give what an untuned batch gives."""
+    sizes = [(96, 96), (64, 160), (130, 70)]
+    outs = []
+    for tune in (True, False):
+        with fg2_b200.Batch(sizes, scheme="hydro", storage="f16") as b:
+            b.config()
+            for k, m in enumerate(b.members):
+                m.init("kh", seed=300 + k)
+            before = [m.download() for m in b.members]
+            if tune:
+                assert b.autotune(reps=1) > 0
+                for x, m in zip(before, b.members):
+                    assert np.array_equal(x, m.download())
+            assert b.advance(4, 1e-4, graph=True) == 0 and b.sync() == 0
+            outs.append([m.download() for m in b.members])
+    for x, y in zip(*outs):
+        assert np.array_equal(x, y)
+
+
 @pytest.mark.parametrize("storage", ["f16", "f64"])
 def test_strip_width_does_not_change_results_of_other_storages(storage, cuda):
     """The 64-column strip with 16-bit deviation storage (its decode pass reads the narrower

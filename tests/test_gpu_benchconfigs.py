@@ -6,6 +6,8 @@
   host core; the port where that build is absent), the loop of src/step.cpp:22-43 around
   src/kick.cu:59-106 and src/drift.cu:21-39.
 * The precision workload's grid: the same layer at 8192^2, 3 steps, against the port.
+* The FP64 kernel the bench's accuracy and precision legs take as truth: the headline layer at
+  4096^2, 3 steps in FP64, against the port in double (relative L2 <= 1e-12).
 * Full-size batch members: the 512-member hydro-isot batch (sides 64..512, box 2 pi) and the
   64-member hydro batch (sides 512..2048), each advanced as one batch; members of the largest
   and smallest sides are compared with the port stepping them alone.
@@ -36,8 +38,8 @@ def oracle(scheme, n1, n2, l1=1.0, l2=1.0, prefer="reference"):
     return o
 
 
-def gpu_steps(n, x, nsteps, dt):
-    with fg2_b200.Sim(n, n) as s:
+def gpu_steps(n, x, nsteps, dt, storage="f32"):
+    with fg2_b200.Sim(n, n, storage=storage) as s:
         s.config()
         s.upload(x)
         t = 0.0
@@ -71,6 +73,18 @@ def test_precision_grid_8192_against_the_port(cuda):
     ref = cpu_steps(oracle("hydro", n, n, prefer="port"), x, nsteps, dt)
     err = rel_l2(gpu, ref)
     assert np.all(err <= 1e-5), err
+
+
+def test_fp64_truth_at_4096_against_the_port(cuda):
+    n, nsteps, dt = 4096, 3, 1.8e-5
+    x = fg2_b200.setup_evaluate("kh", n, n, seed=2)[0]
+    gpu = gpu_steps(n, x, nsteps, dt, storage="f64")
+    o = Oracle("hydro", "f64", "port")
+    o.threads(os.cpu_count() or 1)
+    o.set_delta(1.0 / n, 1.0 / n)
+    ref = cpu_steps(o, x, nsteps, dt)
+    err = rel_l2(gpu, ref)
+    assert np.all(err <= 1e-12), err
 
 
 def batch_members_against_the_port(scheme, sizes, seed_of, box, dt, nsteps, setup):
