@@ -510,7 +510,12 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   }
   std::unique_ptr<void, cudaError_t (*)(void *)> hold(keep, cudaFree);
   std::vector<int> keep_cur;
-  for (fg2_sim *m : b->members) keep_cur.push_back(m->cur);
+  std::vector<char> keep_ghosts, keep_smax;
+  for (fg2_sim *m : b->members) {
+    keep_cur.push_back(m->cur);
+    keep_ghosts.push_back(m->ghosts_valid);
+    keep_smax.push_back(m->smax_valid);
+  }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -545,7 +550,12 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
   if (keep) {
     CK(cudaMemcpyAsync(b->arena, keep, b->arena_bytes, cudaMemcpyDeviceToDevice, b->stream));
     CK(cudaStreamSynchronize(b->stream));
-    for (size_t k = 0; k < b->members.size(); ++k) b->members[k]->cur = keep_cur[k];
+    // the arrays are as they were, ghost cells included: so are the flags that describe them
+    for (size_t k = 0; k < b->members.size(); ++k) {
+      b->members[k]->cur = keep_cur[k];
+      b->members[k]->ghosts_valid = keep_ghosts[k];
+      b->members[k]->smax_valid = keep_smax[k];
+    }
   }
   b->strip = rc ? keep_strip : cands[0].strip;
   b->nb = rc ? keep_nb : cands[0].nb;
