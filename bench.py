@@ -181,7 +181,7 @@ REFERENCE_SWEEP_MS = {1024: 5.468, 1280: 12.136, 1536: 14.992, 1792: 18.016, 204
                       8192: 337.53, 10240: 526.947, 12288: 758.47, 14336: 1036.88}
 
 
-def run_sweep_leg(device, steps=50, warmup=5):
+def run_sweep_leg(device, steps=50, warmup=5, sizes=None):
     """The reference's benchmark sweep re-run here: hydro-isot FP32, periodic 2 pi box, Gaussian
     velocity noise (sigma 0.01, seed 7), the reference's dt, at each of its resolutions
     1024^2 .. 14336^2; steps replayed from the two-step graph, timed with events on the
@@ -190,6 +190,8 @@ def run_sweep_leg(device, steps=50, warmup=5):
     import fg2_b200
     rows = []
     for n, ref_ms in REFERENCE_SWEEP_MS.items():
+        if sizes and n not in sizes:
+            continue
         with fg2_b200.Sim(n, n, scheme="hydro-isot") as s:
             s.config()
             s.init("noise", seed=7)
@@ -813,7 +815,8 @@ def run_fused(args):
         return
     if args.only_sweep:  # the reference's benchmark sweep alone
         torch.cuda.set_device(0)
-        print(json.dumps(run_sweep_leg(torch.device("cuda", 0))), flush=True)
+        sizes = [int(x) for x in args.sweep_sizes.split(",")] if args.sweep_sizes else None
+        print(json.dumps(run_sweep_leg(torch.device("cuda", 0), sizes=sizes)), flush=True)
         return
     if args.only_combined:  # the combined (64-sim FP16 batch) leg alone
         torch.cuda.set_device(0)
@@ -980,6 +983,7 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the reference's benchmark sweep")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP32-against-FP64 error of the headline workload")
     ap.add_argument("--only-sweep", action="store_true", help="run the reference's benchmark sweep alone and print it")
+    ap.add_argument("--sweep-sizes", default="", help="comma-separated sides of the sweep to run (default: all)")
     ap.add_argument("--only-batch", action="store_true", help="run the batch leg alone and print it")
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
