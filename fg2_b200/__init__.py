@@ -40,7 +40,7 @@ def _bind(lib):
         "fg2_scheme_name": (S, []), "fg2_nvar": (I, []), "fg2_field_name": (S, [I]),
         "fg2_eqns_flop": (I, []), "fg2_para_count": (I, []), "fg2_para_key": (S, [I]),
         "fg2_last_error": (S, []),
-        "fg2_setup_evaluate": (I, [S, I, I, D, D, P, U64, P]),
+        "fg2_setup_evaluate": (I, [S, I, I, D, D, P, U64, I, P]),
         "fg2_sim_create": (P, [I, I, I, P]), "fg2_sim_destroy": (None, [P]),
         "fg2_sim_device_bytes": (SZ, [P]), "fg2_sim_storage": (I, [P]),
         "fg2_sim_set_box": (I, [P, D, D]), "fg2_sim_set_courant": (I, [P, D]), "fg2_sim_set_tiling": (I, [P, I]),
@@ -103,8 +103,11 @@ def load_library(scheme="hydro"):
     return _LIBS[scheme]
 
 
-def setup_evaluate(name, n1, n2, scheme="hydro", l1=1.0, l2=1.0, para=None, seed=0):
-    """Evaluate an initial condition on the host: (n1, n2, NVAR) float64 array (no GPU)."""
+def setup_evaluate(name, n1, n2, scheme="hydro", l1=1.0, l2=1.0, para=None, seed=0, storage="f64"):
+    """Evaluate an initial condition on the host: (n1, n2, NVAR) float64 array (no GPU).
+    storage: the precision of the state it is for; with "f32" (or a 16-bit storage) the
+    reference's named setups compute in float, as the reference does with R = float, which is
+    what Sim.init uses for such states."""
     lib = load_library(scheme)
     nv = lib.fg2_nvar()
     out = np.empty((n1, n2, nv), np.float64)
@@ -113,7 +116,7 @@ def setup_evaluate(name, n1, n2, scheme="hydro", l1=1.0, l2=1.0, para=None, seed
         keys = [lib.fg2_para_key(k).decode() for k in range(lib.fg2_para_count())]
         pa = np.array([para[k] for k in keys], np.float64)
     rc = lib.fg2_setup_evaluate(name.encode(), n1, n2, l1, l2, None if pa is None else pa.ctypes.data,
-                                int(seed), out.ctypes.data)
+                                int(seed), STORAGE[storage], out.ctypes.data)
     if rc < 0:
         raise FG2Error(lib.fg2_last_error().decode())
     return out, bool(rc)

@@ -340,16 +340,25 @@ const char *fg2_para_key(int k) { return (k >= 0 && k < scheme::NSLOT) ? scheme:
 const char *fg2_last_error(void) { return g_err; }
 
 int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, const double *para, uint64_t seed,
-                       double *out)
+                       int storage, double *out)
 {
   if (!name || !out || n1 < 1 || n2 < 1) return fail(FG2_ERR_ARG, "bad arguments");
+  const bool single = storage != ST_F64;
   double p[NPARA] = {};
-  for (int q = 0; q < scheme::NSLOT; ++q)
-    p[scheme::PARA_KEYS[q].slot] = para ? para[q] : scheme::PARA_KEYS[q].def;
+  for (int q = 0; q < scheme::NSLOT; ++q) {
+    const double v = para ? para[q] : scheme::PARA_KEYS[q].def;
+    p[scheme::PARA_KEYS[q].slot] = single ? (double)(float)v : v;  // parameters in R (src/para.cpp:34)
+  }
   scheme::derive(p);
   int p1 = BC_PERIODIC, p2 = BC_PERIODIC;
-  scheme::settings<double>(n1, n2, l1, l2, p1, p2);
-  SetupCtx ctx{n1, n2, l1, l2, p, seed};
+  if (single) {  // the box in R, as fg2_sim_set_box keeps it for an FP32 state
+    l1 = (double)(float)l1;
+    l2 = (double)(float)l2;
+    scheme::settings<float>(n1, n2, l1, l2, p1, p2);
+  } else {
+    scheme::settings<double>(n1, n2, l1, l2, p1, p2);
+  }
+  SetupCtx ctx{n1, n2, l1, l2, p, seed, single};
   std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
   const size_t row = (size_t)n2 * scheme::NVAR;
   for (int i = 0; i < n1; ++i) {
@@ -692,7 +701,7 @@ int fg2_sim_init(fg2_sim *s, const char *name, uint64_t seed)
 {
   if (!s || !name) return fail(FG2_ERR_ARG, "null argument");
   ensure_config(s);
-  SetupCtx ctx{s->n1, s->n2, s->l1, s->l2, s->para, seed};
+  SetupCtx ctx{s->n1, s->n2, s->l1, s->l2, s->para, seed, s->storage != ST_F64};
   std::unique_ptr<Setup> setup = scheme::pick(name, ctx);
   const size_t ncell = (size_t)s->n2 * scheme::NVAR;
   std::vector<double> row(ncell, 0.0);

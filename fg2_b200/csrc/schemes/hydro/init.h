@@ -18,7 +18,133 @@ namespace scheme {
 
 namespace detail {
 
-inline double fermi_dirac(double x, double d) { return 1.0 / (std::exp(x / d) + 1.0); }
+// The reference's named setups (blast, bow, implos, KH, Sod) compute in the state's precision
+// R, as src/hydro/init.h:19-99 does with the cell centres of src/init.cpp:30-36: every quantity
+// the reference keeps in an R variable is rounded to R, and the others stay in double, so FP32
+// states agree with the reference's bit for bit (tested against its own header).  eval<R> is
+// instantiated for float (FP32 and 16-bit storage) and double (FP64).
+template <class R>
+R fermi_dirac(R x, R d)
+{
+  return 1.0 / (std::exp(x / d) + 1.0);
+}
+
+struct RefSetup : fg2::Setup {
+  fg2::SetupCtx c;
+  fg2::SetupName nm;
+  fg2::Rng rng;
+  double gamma;
+  RefSetup(const fg2::SetupCtx &ctx, const char *name)
+      : c(ctx), nm(name), rng(ctx.seed), gamma(ctx.para[GAMMA]) {}
+  virtual void eval_f(float x, float y, float *q) = 0;
+  virtual void eval_d(double x, double y, double *q) = 0;
+  template <class R>
+  void fill(int i, double *out)
+  {
+    const R l1 = (R)c.l1, l2 = (R)c.l2;
+    const R x = l1 * (i + 0.5) / c.n1;
+    R q[NVAR];
+    for (int j = 0; j < c.n2; ++j) {
+      const R y = l2 * (j + 0.5) / c.n2;
+      if constexpr (sizeof(R) == 4) eval_f(x, y, q);
+      else eval_d(x, y, q);
+      for (int f = 0; f < NVAR; ++f) out[(size_t)j * NVAR + f] = q[f];
+    }
+  }
+  void row(int i, double *out) override
+  {
+    if (c.single) fill<float>(i, out);
+    else fill<double>(i, out);
+  }
+};
+
+struct Blast : RefSetup {  // src/hydro/init.h:26-34
+  using RefSetup::RefSetup;
+  template <class R>
+  void eval(R x, R y, R *q)
+  {
+    const R g = (R)gamma;
+    x -= 0.5 * (R)c.l1;
+    y -= 0.5 * (R)c.l2;
+    const R e = ((x * x + y * y < 0.01) ? 1.0 : 0.01) / (g - 1.0);
+    q[LND] = 0; q[U1] = 0; q[U2] = 0; q[LNE] = std::log(e);
+  }
+  void eval_f(float x, float y, float *q) override { eval<float>(x, y, q); }
+  void eval_d(double x, double y, double *q) override { eval<double>(x, y, q); }
+};
+
+struct Bow : RefSetup {  // src/hydro/init.h:36-47
+  using RefSetup::RefSetup;
+  template <class R>
+  void eval(R x, R y, R *q)
+  {
+    const R g = (R)gamma;
+    x -= 0.5 * (R)c.l1;
+    y -= 0.5 * (R)c.l2;
+    const R r = std::sqrt(x * x + y * y);
+    const R d = 9.9 * fermi_dirac<R>(r - 0.01, 0.001) + 0.1;
+    const R u = (10.0 / d - 1.0) / 99.0;
+    const R e = 0.01 / d / (g - 1.0);
+    q[LND] = std::log(d); q[U1] = u; q[U2] = 0; q[LNE] = std::log(e);
+  }
+  void eval_f(float x, float y, float *q) override { eval<float>(x, y, q); }
+  void eval_d(double x, double y, double *q) override { eval<double>(x, y, q); }
+};
+
+struct Implos : RefSetup {  // src/hydro/init.h:49-58
+  using RefSetup::RefSetup;
+  template <class R>
+  void eval(R x, R y, R *q)
+  {
+    const R g = (R)gamma;
+    x -= 0.5 * (R)c.l1;
+    y -= 0.5 * (R)c.l2;
+    const double a = 0.15 - std::fabs((double)x) - std::fabs((double)y);
+    const R d = 0.125 + 0.875 * fermi_dirac<R>(a, 0.001);
+    const R p = 0.14 + 0.86 * fermi_dirac<R>(a, 0.001);
+    // the ratio p / d is formed in R, the rest of the quotient and its log in double
+    q[LND] = std::log(d); q[U1] = 0; q[U2] = 0; q[LNE] = (R)std::log(p / d / (g - 1.0));
+  }
+  void eval_f(float x, float y, float *q) override { eval<float>(x, y, q); }
+  void eval_d(double x, double y, double *q) override { eval<double>(x, y, q); }
+};
+
+struct KHStep : RefSetup {  // src/hydro/init.h:60-76 (step profile, +-0.005 noise)
+  using RefSetup::RefSetup;
+  template <class R>
+  void eval(R x, R y, R *q)
+  {
+    (void)x;
+    const R g = (R)gamma;
+    y -= 0.5 * (R)c.l2;
+    const bool in = std::fabs((double)y) < 0.25;
+    const R d = in ? 2.0 : 1.0;
+    const R u = (in ? 0.5 : -0.5) + 0.01 * rng.uniform() - 0.005;
+    const R e = 2.5 / d / (g - 1.0);
+    q[LND] = std::log(d); q[U1] = u; q[U2] = 0; q[LNE] = std::log(e);
+  }
+  void eval_f(float x, float y, float *q) override { eval<float>(x, y, q); }
+  void eval_d(double x, double y, double *q) override { eval<double>(x, y, q); }
+};
+
+struct Sod : RefSetup {  // src/hydro/init.h:78-94
+  using RefSetup::RefSetup;
+  template <class R>
+  void eval(R x, R y, R *q)
+  {
+    const R g = (R)gamma;
+    x -= 0.5 * (R)c.l1;
+    y -= 0.5 * (R)c.l2;
+    // the stripe test in R (x - 2 y + 1.5 mod 1), as the reference writes its literals in R
+    const R t = x - 2 * y + (R)1.5;
+    const bool left = std::fmod((double)t, (double)(R)1.0) < 0.5;
+    const R d = left ? 1.0 : 0.125, P = left ? 1.0 : 0.1;
+    const R e = P / d / (g - 1.0);
+    q[LND] = std::log(d); q[U1] = 0; q[U2] = 0; q[LNE] = std::log(e);
+  }
+  void eval_f(float x, float y, float *q) override { eval<float>(x, y, q); }
+  void eval_d(double x, double y, double *q) override { eval<double>(x, y, q); }
+};
 
 struct PointSetup : fg2::Setup {
   fg2::SetupCtx c;
@@ -32,63 +158,6 @@ struct PointSetup : fg2::Setup {
   {
     const double x = c.l1 * (i + 0.5) / c.n1;
     for (int j = 0; j < c.n2; ++j) cell(x, c.l2 * (j + 0.5) / c.n2, out + (size_t)j * NVAR);
-  }
-};
-
-struct Blast : PointSetup {  // src/hydro/init.h:26-34
-  using PointSetup::PointSetup;
-  void cell(double x, double y, double *q) override
-  {
-    x -= 0.5 * c.l1; y -= 0.5 * c.l2;
-    const double e = ((x * x + y * y < 0.01) ? 1.0 : 0.01) / (gamma - 1.0);
-    q[LND] = 0; q[U1] = 0; q[U2] = 0; q[LNE] = std::log(e);
-  }
-};
-
-struct Bow : PointSetup {  // src/hydro/init.h:36-47
-  using PointSetup::PointSetup;
-  void cell(double x, double y, double *q) override
-  {
-    x -= 0.5 * c.l1; y -= 0.5 * c.l2;
-    const double r = std::sqrt(x * x + y * y);
-    const double d = 9.9 * fermi_dirac(r - 0.01, 0.001) + 0.1;
-    q[LND] = std::log(d); q[U1] = (10.0 / d - 1.0) / 99.0; q[U2] = 0;
-    q[LNE] = std::log(0.01 / d / (gamma - 1.0));
-  }
-};
-
-struct Implos : PointSetup {  // src/hydro/init.h:49-58
-  using PointSetup::PointSetup;
-  void cell(double x, double y, double *q) override
-  {
-    x -= 0.5 * c.l1; y -= 0.5 * c.l2;
-    const double f = fermi_dirac(0.15 - std::fabs(x) - std::fabs(y), 0.001);
-    const double d = 0.125 + 0.875 * f, p = 0.14 + 0.86 * f;
-    q[LND] = std::log(d); q[U1] = 0; q[U2] = 0; q[LNE] = std::log(p / d / (gamma - 1.0));
-  }
-};
-
-struct KHStep : PointSetup {  // src/hydro/init.h:60-76 (step profile, +-0.005 noise)
-  using PointSetup::PointSetup;
-  void cell(double x, double y, double *q) override
-  {
-    (void)x;
-    y -= 0.5 * c.l2;
-    const bool in = std::fabs(y) < 0.25;
-    const double d = in ? 2.0 : 1.0;
-    const double u = (in ? 0.5 : -0.5) + 0.01 * rng.uniform() - 0.005;
-    q[LND] = std::log(d); q[U1] = u; q[U2] = 0; q[LNE] = std::log(2.5 / d / (gamma - 1.0));
-  }
-};
-
-struct Sod : PointSetup {  // src/hydro/init.h:78-94
-  using PointSetup::PointSetup;
-  void cell(double x, double y, double *q) override
-  {
-    x -= 0.5 * c.l1; y -= 0.5 * c.l2;
-    const bool left = std::fmod(x - 2 * y + 1.5, 1.0) < 0.5;
-    const double d = left ? 1.0 : 0.125, P = left ? 1.0 : 0.1;
-    q[LND] = std::log(d); q[U1] = 0; q[U2] = 0; q[LNE] = std::log(P / d / (gamma - 1.0));
   }
 };
 

@@ -73,6 +73,7 @@ struct SetupCtx {
   double l1, l2;
   const double *para;  // the scheme's parameter values by slot
   uint64_t seed;
+  bool single = false;  // the state is FP32 (or 16-bit): the reference's setups compute in float
 };
 
 // Interface of one initial condition: fills row i (n2 cells x NVAR values, cell-interleaved,

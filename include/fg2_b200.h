@@ -61,10 +61,13 @@ const char *fg2_para_key(int k);    /* the para_<key> names of <scheme>/eqns.cuh
 const char *fg2_last_error(void);   /* text of the last library error (thread-local) */
 /* Evaluate a named initial condition on the host (no device needed): fills out[n1*n2*NVAR]
  * in the host layout, in double.  para: the scheme's parameter values in the order of
- * fg2_para_key(), or NULL for the defaults.  Returns 1 for a known name, 0 for an
- * unknown one (zeros, like the reference's pick() default), negative on bad arguments. */
+ * fg2_para_key(), or NULL for the defaults.  storage: the precision of the state it is for
+ * (FG2_F64: double; the others: the reference's setups compute in float, as src/init.cpp with
+ * R = float does, and the parameters and box are rounded to float).  Returns 1 for a known
+ * name, 0 for an unknown one (zeros, like the reference's pick() default), negative on bad
+ * arguments. */
 int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, const double *para, uint64_t seed,
-                       double *out);
+                       int storage, double *out);
 
 /* ---- handle API ------------------------------------------------------------------------ */
 /* setup() (src/setup.cpp:32-87): allocates u (two ping-pong arrays) and v on the current

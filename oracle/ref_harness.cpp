@@ -3,7 +3,8 @@
  *
  * Compiles the reference's OWN per-cell arithmetic for the host: src/fg2.h (types),
  * src/deriv.h (the 6th-order stencil macros), <scheme>/state.h, <scheme>/eqns.cuh
- * (right-hand side), <scheme>/Euler.cuh and <scheme>/bcond.cuh, included in place from
+ * (right-hand side), <scheme>/Euler.cuh, <scheme>/bcond.cuh and, for hydro, <scheme>/init.h
+ * (the named initial conditions, evaluated at cell centres by orc_ref_setup), included in place from
  * the reference tree by oracle/Makefile (-I$(REF)/src -I$(REF)/src/<scheme>).  Nothing
  * of the reference is copied here: this file only provides the host stand-ins for the
  * CUDA qualifiers and the loops (oracle/loops.h), and exports the same C API as
@@ -160,3 +161,37 @@ void orc_deriv(const R *u, int n1, int n2, int which, int field, R *out)
 }
 
 }  // extern "C"
+
+#if defined(FG2_SCHEME_HYDRO)
+// The reference's named initial conditions (src/hydro/init.h, included in place), evaluated at
+// cell centres the way src/init.cpp:26-42 does.  Host stand-ins for the two globals the
+// setups read and for the by-name symbol copy pick() makes of para_gamma.
+namespace global {
+R l1 = 1, l2 = 1;
+}
+static int cudaMemcpyFromSymbol(void *dst, const char *symbol, size_t n)
+{
+  for (const Key &k : keys)
+    if (!std::strncmp(symbol, "para_", 5) && !std::strcmp(symbol + 5, k.name)) {
+      std::memcpy(dst, k.val, n);
+      return 0;
+    }
+  return 1;
+}
+#include <init.h>
+
+extern "C" int orc_ref_setup(const char *name, int n1, int n2, double l1, double l2, R *out)
+{
+  global::l1 = (R)l1;
+  global::l2 = (R)l2;
+  S (*func)(R, R) = pick(name);
+  for (Z i = 0; i < (Z)n1; ++i) {
+    const R x = global::l1 * (i + 0.5) / (Z)n1;
+    for (Z j = 0; j < (Z)n2; ++j) {
+      const R y = global::l2 * (j + 0.5) / (Z)n2;
+      ((S *)out)[i * n2 + j] = func(x, y);
+    }
+  }
+  return 0;
+}
+#endif
