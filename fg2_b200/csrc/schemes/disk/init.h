@@ -4,7 +4,8 @@
 // angular momentum l ~ R^(2 - q0), q0 = 2, pressure maximum at r0 = 16, density 1 and
 // specific energy 0.01 there, inside a static background of density 1e-4 (which co-rotates
 // with sin^2 theta times the torus law); the radiation energy is the background's
-// equilibrium value everywhere.  Evaluated at cell centres (ln(r / r_in), theta), in double.
+// equilibrium value everywhere.  Evaluated at cell centres (ln(r / r_in), theta) in the
+// state's precision.
 //   Hawley  (the reference's only setup; any other name selects it, as src/disk/init.h:60-68
 //           does for every name)
 // Added for benchmarks and tests:
@@ -25,32 +26,39 @@ namespace scheme {
 
 namespace detail {
 
+// The torus in the state's precision R (float for FP32 and 16-bit states), with the
+// reference's roundings: every quantity src/disk/init.h:25-58 keeps in an R variable is rounded
+// to R and the mixed-precision calls (pow of an R and a double) stay in double, so FP32 states
+// agree with the reference's bit for bit (tested against its own header).
 struct Hawley : fg2::Setup {
   fg2::SetupCtx c;
   explicit Hawley(const fg2::SetupCtx &ctx) : c(ctx) {}
-  void row(int i, double *out) override
+  template <class R>
+  void fill(int i, double *out)
   {
-    const double M = c.para[MASS], rin = c.para[RIN], Gamma = c.para[GAMMA], ar = c.para[AR];
-    const double lnr = c.l1 * (i + 0.5) / c.n1;
-    const double q0 = 2.0, r0 = 16.0, d0 = 1.0, e0 = 0.01, bg = 1.0e-4;
-    const double g1 = Gamma - 1.0, q1 = 2.0 * q0 - 2.0;
-    const double lK = std::sqrt(M * std::pow(r0, q1 - 1.0));  // specific angular momentum
-    const double K = g1 * e0 / std::pow(d0, g1);               // polytropic constant
-    const double r = rin * std::exp(lnr);
+    const R M = (R)c.para[MASS], rin = (R)c.para[RIN], Gamma = (R)c.para[GAMMA], ar = (R)c.para[AR];
+    const R l1 = (R)c.l1, l2 = (R)c.l2;
+    const R lnr = l1 * (i + 0.5) / c.n1;
+    const R q0 = 2.0, r0 = 16.0, d0 = 1.0, e0 = 0.01, bg = 0.0001;
+    const R g1 = Gamma - 1.0, q1 = 2.0 * q0 - 2.0;
+    const R lK = std::sqrt(M * std::pow(r0, q1 - 1.0));  // specific angular momentum
+    const R K = (g1 * e0) / std::pow(d0, g1);             // polytropic constant
+    const R r = rin * std::exp(lnr);
     for (int j = 0; j < c.n2; ++j) {
-      const double theta = c.l2 * (j + 0.5) / c.n2;
-      const double R = r * std::sin(theta);
+      const R theta = l2 * (j + 0.5) / c.n2;
+      const R cyl = r * std::sin(theta);
       // Bernoulli constant minus the local potential and centrifugal terms: the enthalpy
-      double h = Gamma * e0 - M / r0 + lK * lK / (std::pow(r0, q1) * q1) + M / r - lK * lK / (std::pow(R, q1) * q1);
-      double den = h > 0.0 ? std::pow(h * g1 / (Gamma * K), 1.0 / g1) : -std::pow(-h * g1 / (Gamma * K), 1.0 / g1);
-      double Omg = lK * std::pow(R, -q0);
+      R den = Gamma * e0 - M / r0 + lK * lK / (std::pow(r0, q1) * q1) + M / r - lK * lK / (std::pow(cyl, q1) * q1);
+      if (den > 0.0) den = std::pow(den * g1 / (Gamma * K), 1.0 / g1);
+      else den = -std::pow(-den * g1 / (Gamma * K), 1.0 / g1);
+      R Omg = lK * std::pow(cyl, -q0);
       if (den < bg) {
         den = bg;
         Omg *= std::sin(theta) * std::sin(theta);
       }
-      const double eng = K * std::pow(den, g1) / g1;
-      const double tbg = K * std::pow(bg, g1);
-      const double rad = ar * tbg * tbg * tbg * tbg / bg;
+      const R eng = K * std::pow(den, g1) / g1;
+      const R tbg = K * std::pow(bg, g1);
+      const R rad = ar * tbg * tbg * tbg * tbg / bg;
       double *q = out + (size_t)j * NVAR;
       q[LND] = std::log(den);
       q[UR] = 0.0;
@@ -59,6 +67,11 @@ struct Hawley : fg2::Setup {
       q[LNE] = std::log(eng);
       q[LNER] = std::log(rad);
     }
+  }
+  void row(int i, double *out) override
+  {
+    if (c.single) fill<float>(i, out);
+    else fill<double>(i, out);
   }
 };
 

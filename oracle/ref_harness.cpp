@@ -3,7 +3,7 @@
  *
  * Compiles the reference's OWN per-cell arithmetic for the host: src/fg2.h (types),
  * src/deriv.h (the 6th-order stencil macros), <scheme>/state.h, <scheme>/eqns.cuh
- * (right-hand side), <scheme>/Euler.cuh, <scheme>/bcond.cuh and, for hydro, <scheme>/init.h
+ * (right-hand side), <scheme>/Euler.cuh, <scheme>/bcond.cuh and, for hydro and disk, <scheme>/init.h
  * (the named initial conditions, evaluated at cell centres by orc_ref_setup), included in place from
  * the reference tree by oracle/Makefile (-I$(REF)/src -I$(REF)/src/<scheme>).  Nothing
  * of the reference is copied here: this file only provides the host stand-ins for the
@@ -162,7 +162,7 @@ void orc_deriv(const R *u, int n1, int n2, int which, int field, R *out)
 
 }  // extern "C"
 
-#if defined(FG2_SCHEME_HYDRO)
+#if defined(FG2_SCHEME_HYDRO) || defined(FG2_SCHEME_DISK)
 // The reference's named initial conditions (src/hydro/init.h, included in place), evaluated at
 // cell centres the way src/init.cpp:26-42 does.  Host stand-ins for the two globals the
 // setups read and for the by-name symbol copy pick() makes of para_gamma.

@@ -178,3 +178,28 @@ def test_named_setups_match_the_reference(name, prec):
     ours = fg2_b200.setup_evaluate(name, n1, n2, seed=1, storage=prec)[0].astype(dtype)
     fields = [0, 2, 3] if name == "KH" else [0, 1, 2, 3]
     assert np.array_equal(ours[..., fields], ref[..., fields])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_disk_torus_matches_the_reference(prec):
+    """The Hawley torus of the disk scheme (src/disk/init.h, compiled for the host) on the
+    scheme's own box, against the library's setup for a state of the same precision, bit for
+    bit."""
+    import ctypes
+    import fg2_b200
+    from oracle.oracle import disk_box, lib_path
+    if not available("disk", prec, "reference"):
+        pytest.skip("reference checker not built here (the reference tree is absent)")
+    lib = ctypes.CDLL(lib_path("disk", prec, "reference"))
+    lib.orc_set_para.argtypes = [ctypes.c_char_p, ctypes.c_double]
+    lib.orc_ref_setup.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_void_p]
+    for key, val in DEFAULTS["disk"].items():
+        lib.orc_set_para(key.encode(), val)
+    n1, n2 = 48, 64
+    l1, l2 = disk_box(n1, n2, prec == "f64")
+    dtype = np.float32 if prec == "f32" else np.float64
+    ref = np.zeros((n1, n2, 6), dtype)
+    lib.orc_ref_setup(b"Hawley", n1, n2, l1, l2, ref.ctypes.data)
+    ours = fg2_b200.setup_evaluate("Hawley", n1, n2, scheme="disk", l1=l1, l2=l2, seed=1, storage=prec)[0]
+    assert np.array_equal(ours.astype(dtype), ref)
