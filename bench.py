@@ -777,7 +777,8 @@ def summary_of(line):
     out = {}
     out["plain_f32"] = {"gcs": line.get("value"), "hbm_frac": g(line, "roofline", "frac"),
                         "e2e_gcs": g(line, "e2e", "value"), "tiling": [g(line, "tiling", "blocks_of_7_rows"),
-                                                                       g(line, "tiling", "ctas_per_sm")]}
+                                                                       g(line, "tiling", "ctas_per_sm"),
+                                                                       g(line, "tiling", "tail_bands")]}
     if line.get("batch"):
         b = line["batch"]
         out["c4_batch"] = {"gcs": b.get("value"), "hbm_frac": g(b, "roofline", "frac"),
@@ -944,7 +945,8 @@ def run_fused(args):
                          "frac_nominal_8tbs": achieved / 8000.0,
                          "bytes_per_cell_step": b_alg, "stage_ms": stage_ms},
             "step_hbm_frac": value / world * b_alg / peak,
-            "tiling": {"blocks_of_7_rows": tiling[0], "ctas_per_sm": tiling[1], "strip_columns": 128,
+            "tiling": {"blocks_of_7_rows": tiling[0], "ctas_per_sm": tiling[1], "tail_bands": tiling[2],
+                       "strip_columns": 128,
                        "how": "--tiling" if args.tiling else "fg2_sim_autotune on the workload's own state"},
             "cpu_baseline": cpu,
             "accuracy_vs_f64": accuracy,
@@ -988,7 +990,7 @@ def main():
     ap.add_argument("--batch-tiling", default="",
                     help="nb,ctas_per_sm[,strip] for the batch leg (default: autotune)")
     ap.add_argument("--tiling", default="",
-                    help="nb,ctas_per_sm of the headline workload's launches (default: autotune)")
+                    help="nb,ctas_per_sm[,tail_bands] of the headline workload's launches (default: autotune)")
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
                     help="state storage of the headline workload (f16/bf16: deviation storage)")
     args = ap.parse_args()

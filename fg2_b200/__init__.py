@@ -45,7 +45,9 @@ def _bind(lib):
         "fg2_sim_device_bytes": (SZ, [P]), "fg2_sim_storage": (I, [P]),
         "fg2_sim_set_box": (I, [P, D, D]), "fg2_sim_set_courant": (I, [P, D]), "fg2_sim_set_tiling": (I, [P, I]),
         "fg2_sim_set_occupancy": (I, [P, I]), "fg2_sim_get_tiling": (I, [P, ctypes.POINTER(I), ctypes.POINTER(I)]),
-        "fg2_sim_autotune": (I, [P, I, ctypes.POINTER(D)]),
+        "fg2_sim_autotune": (I, [P, I, ctypes.POINTER(D)]), "fg2_sim_set_tail": (I, [P, I]),
+        "fg2_tile_bands": (I, [I, I, I, I, ctypes.POINTER(I), I]),
+        "fg2_sim_get_tail": (I, [P, ctypes.POINTER(I)]),
         "fg2_sim_set_bcond": (I, [P, I, I]), "fg2_sim_para": (S, [P, S]),
         "fg2_sim_get_para": (I, [P, S, ctypes.POINTER(D)]), "fg2_sim_config": (I, [P]),
         "fg2_sim_init": (I, [P, S, U64]), "fg2_sim_upload": (I, [P, P]), "fg2_sim_download": (I, [P, P]),
@@ -122,6 +124,18 @@ def setup_evaluate(name, n1, n2, scheme="hydro", l1=1.0, l2=1.0, para=None, seed
     return out, bool(rc)
 
 
+def tile_bands(n1, nb=0, tail=0, reverse=False, scheme="hydro"):
+    """The row bands (i0, iend, blocks) the fused kernel cuts a grid of n1 rows into, in the
+    order a launch takes them (host only, no GPU)."""
+    lib = load_library(scheme)
+    n = lib.fg2_tile_bands(int(n1), int(nb), int(tail), int(reverse), None, 0)
+    if n < 0:
+        raise FG2Error("bad tile band arguments")
+    out = (ctypes.c_int * (3 * max(n, 1)))()
+    lib.fg2_tile_bands(int(n1), int(nb), int(tail), int(reverse), out, n)
+    return [tuple(out[3 * q:3 * q + 3]) for q in range(n)]
+
+
 class Sim:
     """One simulation on the current CUDA device (the handle API, fg2_sim_*)."""
 
@@ -181,18 +195,22 @@ class Sim:
     def set_courant(self, c):
         self._check(self.lib.fg2_sim_set_courant(self.h, c), "set_courant")
 
-    def set_tiling(self, nb, ctas_per_sm=None):
+    def set_tiling(self, nb, ctas_per_sm=None, tail=None):
         """Tile height of the fused kernel in blocks of 7 rows (0: the default) and, if given,
-        CTAs per SM of its persistent grid (0: as many as fit)."""
+        CTAs per SM of its persistent grid (0: as many as fit) and the number of one-block
+        tail bands that end the grid (0: none)."""
         self._check(self.lib.fg2_sim_set_tiling(self.h, int(nb)), "set_tiling")
         if ctas_per_sm is not None:
             self._check(self.lib.fg2_sim_set_occupancy(self.h, int(ctas_per_sm)), "set_occupancy")
+        if tail is not None:
+            self._check(self.lib.fg2_sim_set_tail(self.h, int(tail)), "set_tail")
 
     def tiling(self):
-        """(tile height in blocks of 7 rows, CTAs per SM) the launches use."""
-        nb, c = ctypes.c_int(), ctypes.c_int()
+        """(tile height in blocks of 7 rows, CTAs per SM, tail bands) the launches use."""
+        nb, c, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(self.lib.fg2_sim_get_tiling(self.h, ctypes.byref(nb), ctypes.byref(c)), "tiling")
-        return nb.value, c.value
+        self._check(self.lib.fg2_sim_get_tail(self.h, ctypes.byref(t)), "tiling")
+        return nb.value, c.value, t.value
 
     def autotune(self, reps=3):
         """Time every tiling candidate on this simulation's state (left unchanged) and keep the

@@ -39,7 +39,7 @@ struct fg2_batch {
   Status *status = nullptr;        // device, one per member
   Status *status_host = nullptr;   // pinned mirror
   std::vector<fg2_sim *> members;
-  std::vector<int> order;          // members in tile order (descending cell count)
+  std::vector<int> order;          // members in tile order (smallest at both ends)
   long long cells = 0;
   GridDesc *desc = nullptr;        // device [2][count]: set 0 u[cur] -> u[1-cur], set 1 the reverse
   std::vector<GridDesc> desc_host;
@@ -280,11 +280,16 @@ fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage
     b->members.push_back(m);
     p += na * bytes[k];
   }
-  b->order.resize(count);
-  for (int k = 0; k < count; ++k) b->order[k] = k;
-  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
-    return (long long)n1[x] * n2[x] > (long long)n1[y] * n2[y];
+  // tile order: the smallest members at both ends and the largest in the middle, so that
+  // launches in either direction (they alternate) end on short tiles of small members and
+  // the persistent CTAs finish together
+  std::vector<int> by_size(count);
+  for (int k = 0; k < count; ++k) by_size[k] = k;
+  std::stable_sort(by_size.begin(), by_size.end(), [&](int x, int y) {
+    return (long long)n1[x] * n2[x] < (long long)n1[y] * n2[y];
   });
+  b->order.resize(count);
+  for (int r = 0, front = 0, back = count - 1; r < count; ++r) b->order[(r & 1) ? back-- : front++] = by_size[r];
   b->desc_host.resize(2 * (size_t)count);
   b->limits_host.resize(count);
   b->versions.assign(count, 0);

@@ -91,6 +91,7 @@ struct KParams {
   const double *dt_dev;  // device time step for grids without their own, or null: dt
   Status *status;        // launch errors
   int nb;                // output blocks of 7 rows per tile
+  int tail;              // one-block bands that at least end each grid (0: none)
   int strip;             // strip width (columns per tile, threads per CTA)
   int reverse;           // tiles last first
   unsigned wait_test_bytes;  // extra bytes every chunk expects (timeout-path tests; 0 otherwise)
@@ -149,6 +150,7 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.dt_dev = a.dt_dev;
   kp.status = a.status;
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
+  kp.tail = a.tail > 0 ? a.tail : 0;
   kp.strip = strip_width(a.strip);
   kp.comp_bg = a.comp_bg;
   kp.reverse = a.reverse;
@@ -302,9 +304,27 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
 
 int strip_width(int strip) { return strip == 64 ? 64 : STRIP_DEFAULT; }
 
-int substage_tiles(const Layout &L, int nb, int strip)
+int substage_tiles(const Layout &L, int nb, int strip, int tail)
 {
-  return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT, strip_width(strip)).ntiles;
+  return sub::tile_grid(L, nb > 0 ? nb : sub::NB_DEFAULT, strip_width(strip), tail > 0 ? tail : 0).ntiles;
+}
+
+int tile_bands(int n1, int nb, int tail, int reverse, int *out, int cap)
+{
+  if (n1 < 1 || nb < 0 || tail < 0) return -1;
+  Layout L{};
+  L.n1 = n1;
+  L.n2 = 1;
+  const int h = nb > 0 ? nb : sub::NB_DEFAULT;
+  const sub::TileGrid g = sub::tile_grid(L, h, STRIP_DEFAULT, tail);
+  const int nbands = g.bands + g.small;
+  for (int q = 0; q < nbands && q < cap; ++q) {
+    const sub::Band b = sub::band_rows(n1, h, g.bands, q, reverse != 0);
+    out[3 * q] = b.i0;
+    out[3 * q + 1] = b.iend;
+    out[3 * q + 2] = b.nbt;
+  }
+  return nbands;
 }
 
 template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC, int W>

@@ -25,6 +25,8 @@ struct StageArgs {
   int p1, p2;           // boundary kind per axis (BC_PERIODIC / BC_WALL)
   Status *status;       // device status block (launch errors; per-grid blocks are in GridDesc)
   int nb = 0;           // tile height in blocks of 7 rows (0: the default)
+  int tail = 0;         // the last rows of each grid as at least this many one-block tiles,
+                        // so a launch's last tiles are short (0: none)
   int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
   int strip = 0;        // strip width: 64 or 128 columns per tile (0: 128); one thread per
                         // column, so 2 or 4 warps per CTA; the descriptors must match it
@@ -75,8 +77,12 @@ constexpr int TILE_BLOCKS_DEFAULT = 4;
 // Strip width of single-grid launches; batch launches may also use 64 (strip_width(64)).
 constexpr int STRIP_DEFAULT = 128;
 int strip_width(int strip);
-// Tiles of one grid for a tile height of nb blocks of 7 rows and a strip width (0: defaults).
-int substage_tiles(const Layout &L, int nb = 0, int strip = 0);
+// Tiles of one grid for a tile height of nb blocks of 7 rows, a strip width and a number of
+// one-block tail bands (0: defaults, no tail bands).
+int substage_tiles(const Layout &L, int nb = 0, int strip = 0, int tail = 0);
+// The row bands of a grid of n1 rows in the fused kernel's processing order (reverse: a
+// reverse launch's), as (i0, iend, blocks) triples into out[3 cap]; returns the band count.
+int tile_bands(int n1, int nb, int tail, int reverse, int *out, int cap);
 
 // One fused substage over the grids of `grids` (device array of ngrids descriptors holding
 // ntiles tiles in all).  `scaled`: the grids differ in Delta (stencil weights scaled per grid);

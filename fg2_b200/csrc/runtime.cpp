@@ -118,6 +118,7 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.comp_bg = k == 1 ? RK_BETA[2] * RK_GAMMA[2] : 0.0;  // 16-bit stage 1 folds its residual into v
   a.wait_test_bytes = s->wait_test_bytes;
   a.nb = tile_height(s);
+  a.tail = s->tail;
   a.max_ctas = s->max_ctas;
   return a;
 }
@@ -145,7 +146,8 @@ int launch_stage(fg2_sim *s, int kind, bool cfl, const StageArgs &a, const GridD
   StageArgs b = a;
   b.reverse = s->order;
   s->order ^= 1;
-  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L, b.nb), b, s->queue, s->stream));
+  CK(launch_substage(s->storage, kind, cfl, false, desc, 1, substage_tiles(s->L, b.nb, 0, b.tail), b, s->queue,
+                             s->stream));
   return FG2_OK;
 }
 
@@ -338,6 +340,10 @@ int fg2_eqns_flop(void) { return scheme::EQNS_FLOP; }
 int fg2_para_count(void) { return scheme::NSLOT; }
 const char *fg2_para_key(int k) { return (k >= 0 && k < scheme::NSLOT) ? scheme::PARA_KEYS[k].name : nullptr; }
 const char *fg2_last_error(void) { return g_err; }
+int fg2_tile_bands(int n1, int nb, int tail, int reverse, int *out, int cap)
+{
+  return tile_bands(n1, nb, tail, reverse, out, out ? cap : 0);
+}
 
 int fg2_setup_evaluate(const char *name, int n1, int n2, double l1, double l2, const double *para, uint64_t seed,
                        int storage, double *out)
@@ -550,6 +556,21 @@ int fg2_sim_set_occupancy(fg2_sim *s, int ctas_per_sm)
   return FG2_OK;
 }
 
+int fg2_sim_set_tail(fg2_sim *s, int tail)
+{
+  if (!s || tail < 0 || tail > 64) return fail(FG2_ERR_ARG, "bad tail band count %d", tail);
+  if (tail != s->tail) drop_graph(s);
+  s->tail = tail;
+  return FG2_OK;
+}
+
+int fg2_sim_get_tail(const fg2_sim *s, int *tail)
+{
+  if (!s || !tail) return fail(FG2_ERR_ARG, "null argument");
+  *tail = s->tail;
+  return FG2_OK;
+}
+
 int fg2_sim_get_tiling(const fg2_sim *s, int *nb, int *ctas_per_sm)
 {
   if (!s) return fail(FG2_ERR_ARG, "null handle");
@@ -563,14 +584,18 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   if (!s || reps < 1) return fail(FG2_ERR_ARG, "bad arguments");
   ensure_config(s);
   struct Cand {
-    int nb, ctas;
+    int nb, ctas, tail;
     double ms;
   };
   std::vector<Cand> cands;
-  // tile height nb blocks of 7 rows; CTAs per SM: 0 = as many as fit, or 4, 8, 12 warps
+  // tile height nb blocks of 7 rows; CTAs per SM: 0 = as many as fit, or 4, 8, 12 warps;
+  // one-block tail bands: none, 1 or 3 (a tail only changes grids with more than one band)
   for (int nb : {1, 2, 3, 4, 5, 6, 8})
-    for (int warps : {0, 4, 8, 12}) cands.push_back({nb, warps * 32 / STRIP_DEFAULT, 0.0});
-  const int keep_nb = s->nb, keep_ctas = s->max_ctas, keep_cur = s->cur;
+    for (int warps : {0, 4, 8, 12})
+      for (int tail : {0, 1, 3})
+        if (tail == 0 || (nb > 1 && substage_tiles(s->L, nb, 0, tail) != substage_tiles(s->L, nb)))
+          cands.push_back({nb, warps * 32 / STRIP_DEFAULT, tail, 0.0});
+  const int keep_nb = s->nb, keep_ctas = s->max_ctas, keep_tail = s->tail, keep_cur = s->cur;
   const bool keep_ghosts = s->ghosts_valid, keep_smax = s->smax_valid;
   // 16-bit storage: a step of dt = 0 re-encodes the state and drops its rounding residual, so
   // the state and the residual are kept aside and put back afterwards
@@ -588,6 +613,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   auto measure = [&](Cand &c) -> int {
     s->nb = c.nb;
     s->max_ctas = c.ctas;
+    s->tail = c.tail;
     int r = FG2_OK;
     // two untimed steps, then 2 reps timed (dt = 0: u' = u + 0 v, bitwise)
     for (int q = 0; q < 2 && r == 0; ++q) r = enqueue_step(s, 0.0, nullptr, false);
@@ -606,7 +632,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   // which no tiling changes and which hides the kernel's own time, so such grids keep the
   // default (its small-grid rule gives every resident CTA a tile)
   constexpr double LAUNCH_BOUND_MS = 0.05;
-  Cand dflt{0, 0, 0.0};
+  Cand dflt{0, 0, 0, 0.0};
   int rc = measure(dflt);
   const bool launch_bound = rc == 0 && dflt.ms < LAUNCH_BOUND_MS;
   if (launch_bound) cands.assign(1, dflt);
@@ -634,6 +660,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   s->smax_valid = keep_smax;  // the state is unchanged
   s->nb = rc ? keep_nb : cands[0].nb;
   s->max_ctas = rc ? keep_ctas : cands[0].ctas;
+  s->tail = rc ? keep_tail : cands[0].tail;
   drop_graph(s);
   if (rc) return rc;
   if (best_ms) *best_ms = cands[0].ms;

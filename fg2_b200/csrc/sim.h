@@ -35,6 +35,7 @@ struct fg2_sim {
   int order = 0;              // tile order of the next substage launch (alternates)
   int nb = 0;                 // tile height in blocks of 7 rows (0: the default)
   int max_ctas = 0;           // CTAs per SM of the persistent grid (0: as many as fit)
+  int tail = 0;               // one-block tail bands ending the grid (0: none)
   unsigned wait_test_bytes = 0;  // timeout-path tests (fg2_sim_test_stall_waits)
   int *queue = nullptr;   // tile queue of the substage kernel (self-resetting)
   cudaStream_t stream = nullptr;

@@ -4,9 +4,12 @@
 // Work decomposition.  A launch advances a list of grids (one simulation, or a batch of
 // independent simulations of any sizes).  A tile is a strip of W interior columns (128, or
 // 64 in batch launches) by 7 nb rows of one grid (nb blocks of 7 output rows, a launch
-// parameter, 4 by default); the launch's tiles are numbered grid by grid, strip fastest, and
-// a persistent grid of CTAs drains them from a queue (an atomic counter that the last CTA to
-// finish resets, so a launch needs no host-side reset and replays from a CUDA graph).  A CTA
+// parameter, 4 by default; the launch's `tail` parameter makes the last rows of each grid
+// one-block tiles, and a band cut by the grid's edge has fewer blocks); the launch's tiles
+// are numbered grid by grid, strip fastest, and a persistent grid of CTAs drains them from a
+// queue (an atomic counter that the last CTA to finish resets, so a launch needs no host-side
+// reset and replays from a CUDA graph).  Launches alternate direction: a reverse launch takes
+// the grids last first and lays each grid's bands out from its last row up.  A CTA
 // has W / 32 warps; a thread owns one column of the strip.  Each grid is described by a GridDesc in
 // device memory: its TMA tensor maps, output pointers, layout, boundaries, time step and
 // status block.
@@ -113,8 +116,9 @@ struct Geo {
   static constexpr size_t DEC_ONE = DEV ? ((size_t)BW * CH * NV * sizeof(float) + 127) / 128 * 128 : 0;
   static constexpr size_t DEC_BYTES = 2 * DEC_ONE;
   static constexpr size_t BAR_OFF = DEC_OFF + DEC_BYTES;
-  // tail: full[NSLOT] (mbarriers), tile_of[NSLOT], grid_of[NSLOT], producer state
-  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + 2 * NSLOT * sizeof(int) + 8 * sizeof(int) + 64;
+  // tail: full[NSLOT] (mbarriers), the slots' tiles (TileSlot, 6 ints each), producer state
+  // (Producer, 12 ints)
+  static constexpr size_t SMEM = BAR_OFF + NSLOT * sizeof(uint64_t) + NSLOT * 6 * sizeof(int) + 12 * sizeof(int) + 64;
   static_assert(SLOT % 128 == 0, "TMA shared-memory boxes must be 128-byte aligned");
   static_assert(BW % G == 0 && VBW % G == 0 && (GL - VOFF) % G == 0, "boxes and tile origins are whole cell groups");
   static_assert(BW / G <= 256 && VBW / G <= 256 && CH <= 256 && G * NV <= 256, "TMA box dimensions");
@@ -239,20 +243,62 @@ __device__ __forceinline__ int source_index(int i, int n, int periodic)
 }
 
 // Tiles of one grid: strip fastest, so horizontally adjacent tiles run together and share
-// their halo columns through L2.
+// their halo columns through L2.  The rows are cut into `bands` bands of nb blocks of 7 rows
+// and then `small` tail bands of one block: with tail > 0 at least `tail` one-block bands end
+// the grid, so the last tiles a launch hands out are short and the CTAs finish together
+// (the persistent grid's last wave would otherwise be whole tiles on a few CTAs).  tail = 0:
+// nb-block bands only, the last one cut at the grid's edge.
 struct TileGrid {
-  int strips, rows, ntiles;
+  int strips, bands, small, ntiles;
 };
 
-__host__ __device__ inline TileGrid tile_grid(const Layout &L, int nb, int sw)
+__host__ __device__ inline TileGrid tile_grid(const Layout &L, int nb, int sw, int tail = 0)
 {
   TileGrid g;
   const int th = nb * CH;
   g.strips = (L.n2 + sw - 1) / sw;
-  g.rows = (L.n1 + th - 1) / th;
-  g.ntiles = g.strips * g.rows;
+  if (tail > 0) {
+    const int b = (L.n1 - CH * tail) / th;
+    g.bands = b > 0 ? b : 0;
+  } else {
+    g.bands = (L.n1 + th - 1) / th;
+  }
+  const int rest = L.n1 - g.bands * th;
+  g.small = rest > 0 ? (rest + CH - 1) / CH : 0;
+  g.ntiles = g.strips * (g.bands + g.small);
   return g;
 }
+
+// Rows of the band at processing position q of a grid: the nb-block bands first, then the
+// one-block tail bands.  A reverse launch lays the bands out from the last row up, so it too
+// takes the tail bands last; the band that meets the grid's far edge is cut there.  A tile
+// computes rows [i0, iend) in nbt blocks (its last block may reach past iend: those rows
+// belong to the next band or lie past the grid, and are not written).
+struct Band {
+  int i0, iend, nbt;
+};
+__host__ __device__ inline Band band_rows(int n1, int nb, int bands, int q, bool reverse)
+{
+  const int th = nb * CH;
+  const int len = q < bands ? th : CH;
+  const int off = q < bands ? q * th : bands * th + (q - bands) * CH;
+  Band b;
+  if (!reverse) {
+    b.i0 = off;
+    b.iend = off + len < n1 ? off + len : n1;
+  } else {
+    b.iend = n1 - off;
+    b.i0 = b.iend - len > 0 ? b.iend - len : 0;
+  }
+  b.nbt = (b.iend - b.i0 + CH - 1) / CH;
+  return b;
+}
+
+// The tile a chunk slot holds, written by the issuing thread with the slot's first chunk:
+// launch tile (< 0: the end of the queue), grid, rows [i0, iend) in nbt blocks, first column.
+struct TileSlot {
+  int tile, g, i0, iend, j0, nbt;
+};
 
 // Does field f carry second derivatives (D11, D22) under mask M2?
 template <unsigned M2>
@@ -527,7 +573,7 @@ __device__ __noinline__ void rim_images_raw(S *u, const Layout L, int i, int j, 
 // 2 reads once, with no carry beyond it.  The stencil itself reads S.
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP],
-                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j,
+                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j, int iend,
                                          const float4 &scv, const float4 &ivv,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
                                          const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
@@ -552,7 +598,7 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   T r[NV];
   const T dl1 = SC ? gr.delta1 : a.ks.delta1, dl2 = SC ? gr.delta2 : a.ks.delta2;
   scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2, cg);
-  if (!full && (i >= gr.L.n1 || j >= gr.L.n2)) return;  // cells past the grid (partial tiles)
+  if (!full && (i >= iend || j >= gr.L.n2)) return;  // cells past the tile's rows or the grid
   P sc[NP], iv[NP];  // deviation storage: the scales of the cell's tile
   if constexpr (DEV && WRITE_U) {
     sc[0] = make_float2(scv.x, scv.y);
@@ -621,13 +667,12 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
 
 // Shared state of the chunk issue, read and written by thread 0 only.
 struct Producer {
-  int next_n;  // index of the next chunk to issue
-  int tile;    // launch tile of that chunk
-  int g;       // its grid
-  int i0, j0;  // its origin in the grid
-  int c;       // chunk index within the tile (0 = warm-up)
-  int done;    // the end-of-queue sentinel was issued
+  int next_n;    // index of the next chunk to issue
+  int c;         // chunk index within the tile (0 = warm-up)
+  int done;      // the end-of-queue sentinel was issued
+  TileSlot cur;  // the tile of that chunk
 };
+static_assert(sizeof(TileSlot) == 6 * sizeof(int) && sizeof(Producer) <= 12 * sizeof(int), "shared-memory tail");
 
 // Grid of launch tile t: the last grid whose first tile is <= t (grids are in tile order).
 __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, int t)
@@ -646,8 +691,8 @@ __device__ __forceinline__ int grid_of_tile(const GridDesc *grids, int ngrids, i
 // it is drawn when the last chunk of the current tile is issued, one chunk before it is
 // needed, so the atomic's round trip is off the chunk's critical path.
 template <class S, bool READ_V, bool READ_R, int W>
-__device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, int *tile_of,
-                                            int *grid_of, const GridDesc *grids, int ngrids, int ntiles, int nb,
+__device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, uint64_t *full, TileSlot *slots,
+                                            const GridDesc *grids, int ngrids, int ntiles, int nb, int tail,
                                             bool reverse, unsigned extra_bytes, int *queue, int &claim)
 {
   using G = Geo<S, READ_V, READ_R, W>;
@@ -657,23 +702,25 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     int t = claim;
     if (t >= ntiles) t = -1;
     else if (reverse) t = ntiles - 1 - t;
-    ps->tile = t;
-    tile_of[s] = t;
+    TileSlot ts{t, 0, 0, 0, 0, 0};
     if (t >= 0) {
       const int g = grid_of_tile(grids, ngrids, t);
-      const int local = t - grids[g].tile0, strips = grids[g].strips;
-      ps->g = g;
-      ps->i0 = (local / strips) * (nb * CH);
-      ps->j0 = (local % strips) * W;
-      grid_of[s] = g;
+      const GridDesc &gd = grids[g];
+      const TileGrid tg = tile_grid(gd.L, nb, W, tail);
+      int q = t - gd.tile0;                // position of the tile in the grid's processing order
+      if (reverse) q = tg.ntiles - 1 - q;
+      const Band bd = band_rows(gd.L.n1, nb, tg.bands, q / tg.strips, reverse);
+      ts = TileSlot{t, g, bd.i0, bd.iend, (q % tg.strips) * W, bd.nbt};
     }
+    ps->cur = ts;
+    slots[s] = ts;
   }
-  if (ps->tile < 0) {
+  if (ps->cur.tile < 0) {
     mbar_arrive(&full[s]);
     ps->done = 1;
   } else {
-    const GridDesc &gd = grids[ps->g];
-    const int i0 = ps->i0, j0 = ps->j0, c = ps->c;
+    const GridDesc &gd = grids[ps->cur.g];
+    const int i0 = ps->cur.i0, j0 = ps->cur.j0, c = ps->c, last = ps->cur.nbt;
     const bool with_v = READ_V && c > 0, with_r = READ_R && c > 0;
     mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + (with_r ? G::V_BYTES : 0u) + extra_bytes);
     // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
@@ -687,8 +734,8 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     if (with_r)
       tma_load_3d(smem + (size_t)s * G::SLOT + G::R_OFF, &gd.tm_r, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
                   i0 + CH * (c - 1) + GT);
-    if (c == nb) claim = atomicAdd(&queue[0], 1);  // the next tile's position, used one chunk later
-    ps->c = c == nb ? 0 : c + 1;
+    if (c == last) claim = atomicAdd(&queue[0], 1);  // the next tile's position, used one chunk later
+    ps->c = c == last ? 0 : c + 1;
   }
   ps->next_n = n + 1;
 }
@@ -802,33 +849,35 @@ struct TileState {
   GridRegs<S> gr;
   int cur_g = -1;
   int i0 = 0, j0 = 0, b = -1;      // tile origin and block (-1: the warm-up chunk)
+  int iend = 0, nbt = 0;           // the tile's rows end before iend; its blocks
   int tj = 0;                      // scale-tile column of the thread's column (16-bit storage)
   bool whole = false, rim = true;  // the tile lies inside the grid / within HALF cells of an edge
   scheme::Geom<T> cg{};            // the scheme's geometry of the thread's column
 };
 
-// Enters launch tile `tile` of grid g (warp-uniform call: flushes the previous grid's NaN
-// flag and CFL max with warp collectives when the grid changes).
+// Enters the tile of a chunk slot (warp-uniform call: flushes the previous grid's NaN flag
+// and CFL max with warp collectives when the grid changes).
 template <class S, bool WRITE_U, bool CFL, bool SC, int W>
-__device__ __forceinline__ void enter_tile(TileState<S> &ts, const GridDesc *grids, int g, int tile,
+__device__ __forceinline__ void enter_tile(TileState<S> &ts, const GridDesc *grids, const TileSlot &slot,
                                            const KParams<typename Store<S>::C> &a, bool &nan,
                                            typename Store<S>::C &rate)
 {
   using T = typename Store<S>::C;
+  const int g = slot.g;
   if (g != ts.cur_g) {
     if (ts.cur_g >= 0) flush_grid<WRITE_U, CFL>(ts.gr.status, nan, rate);
     load_grid<S, SC>(grids[g], a, ts.gr);
     ts.cur_g = g;
   }
-  const int local = tile - grids[g].tile0, strips = grids[g].strips;
-  const int th = a.nb * CH;
-  ts.i0 = (local / strips) * th;
-  ts.j0 = (local % strips) * W;
+  ts.i0 = slot.i0;
+  ts.iend = slot.iend;
+  ts.j0 = slot.j0;
+  ts.nbt = slot.nbt;
   ts.b = -1;
   const int j = ts.j0 + (int)threadIdx.x;
-  ts.whole = ts.i0 + th <= ts.gr.L.n1 && ts.j0 + W <= ts.gr.L.n2;
+  ts.whole = ts.iend - ts.i0 == CH * ts.nbt && ts.j0 + W <= ts.gr.L.n2;
   ts.cg = scheme::column_geom<T>(j, SC ? ts.gr.delta2 : a.ks.delta2);
-  ts.rim = ts.i0 < HALF || ts.i0 + th > ts.gr.L.n1 - HALF || ts.j0 < HALF || ts.j0 + W > ts.gr.L.n2 - HALF;
+  ts.rim = ts.i0 < HALF || ts.iend > ts.gr.L.n1 - HALF || ts.j0 < HALF || ts.j0 + W > ts.gr.L.n2 - HALF;
   if constexpr (Store<S>::DEV) ts.tj = min(j, ts.gr.L.n2 - 1) >> 6;
 }
 
@@ -884,8 +933,8 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
       ivv = __ldg(ts.gr.inv + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);                                \
     }                                                                                                      \
     lead_row<T, M2, R, BW * NV>(base, a, st);                                                              \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, scv, ivv, a, ts.gr, st,    \
-                                                          ts.whole, ts.rim, nan, rate, ts.cg);             \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, ts.iend, scv, ivv, a, ts.gr, \
+                                                          st, ts.whole, ts.rim, nan, rate, ts.cg);         \
   }
     FG2_ROW(0) FG2_ROW(1) FG2_ROW(2) FG2_ROW(3) FG2_ROW(4) FG2_ROW(5) FG2_ROW(6)
 #undef FG2_ROW
@@ -923,22 +972,20 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + G::BAR_OFF);
-  int *tile_of = reinterpret_cast<int *>(full + NS);
-  int *grid_of = tile_of + NS;
-  Producer *ps = reinterpret_cast<Producer *>(grid_of + NS);
+  TileSlot *slots = reinterpret_cast<TileSlot *>(full + NS);
+  Producer *ps = reinterpret_cast<Producer *>(slots + NS);
 
   int claim = 0;  // issuing thread: queue position of the CTA's next tile
   if (threadIdx.x == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
     fence_mbar_init();
     ps->next_n = 0;
-    ps->tile = -1;
-    ps->g = 0;
     ps->c = 0;
     ps->done = 0;
+    ps->cur = TileSlot{-1, 0, 0, 0, 0, 0};
     claim = atomicAdd(&queue[0], 1);
     for (int s = 0; s < NS; ++s)
-      issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+      issue_chunk<S, READ_V, RR, W>(ps, smem, full, slots, grids, ngrids, ntiles, a.nb, a.tail, a.reverse != 0,
                                     a.wait_test_bytes, queue, claim);
   }
   __syncthreads();
@@ -956,14 +1003,13 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
   // the tile state for chunk n: a new tile after the last block of the previous one (tile < 0:
   // the end of the queue); returns false at the end
   auto advance = [&](int n) {
-    if (ts.cur_g >= 0 && ts.b < a.nb - 1) {  // the next block of the current tile
+    if (ts.cur_g >= 0 && ts.b < ts.nbt - 1) {  // the next block of the current tile
       ++ts.b;
       return true;
     }
-    const int s = n % NS;
-    const int tile = tile_of[s];
-    if (tile < 0) return false;
-    enter_tile<S, WRITE_U, CFL, SC, W>(ts, grids, grid_of[s], tile, a, nan, rate);
+    const TileSlot &slot = slots[n % NS];
+    if (slot.tile < 0) return false;
+    enter_tile<S, WRITE_U, CFL, SC, W>(ts, grids, slot, a, nan, rate);
     return true;
   };
   bool failed = false;
@@ -984,7 +1030,7 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
       }
       if (!live) break;  // the end of the queue (the same chunk for every thread)
       if (threadIdx.x == 0)
-        issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+        issue_chunk<S, READ_V, RR, W>(ps, smem, full, slots, grids, ngrids, ntiles, a.nb, a.tail, a.reverse != 0,
                                       a.wait_test_bytes, queue, claim);  // refill chunk n's slot
     }
   } else {
@@ -1009,7 +1055,7 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
       }
       failed = __syncthreads_or(!landed);
       if (!failed && live && threadIdx.x == 0)
-        issue_chunk<S, READ_V, RR, W>(ps, smem, full, tile_of, grid_of, grids, ngrids, ntiles, a.nb, a.reverse != 0,
+        issue_chunk<S, READ_V, RR, W>(ps, smem, full, slots, grids, ngrids, ntiles, a.nb, a.tail, a.reverse != 0,
                                       a.wait_test_bytes, queue, claim);  // refill chunk n's slot
     }
   }

@@ -88,8 +88,19 @@ int fg2_sim_set_tiling(fg2_sim *s, int nb);
  * tiling (the tile height the launches use, after the default's small-grid rule). */
 int fg2_sim_set_occupancy(fg2_sim *s, int ctas_per_sm);
 int fg2_sim_get_tiling(const fg2_sim *s, int *nb, int *ctas_per_sm);
+/* Tail bands: the last rows of the grid are cut into at least `tail` tiles of one block of 7
+ * rows (0: none, the default), so that the last tiles of a launch's queue are short and the
+ * persistent CTAs finish together.  Results are bitwise the same for every value. */
+int fg2_sim_set_tail(fg2_sim *s, int tail);
+int fg2_sim_get_tail(const fg2_sim *s, int *tail);
+/* The row bands the fused kernel cuts a grid of n1 rows into for tile height nb (0: the
+ * default) and `tail` tail bands, in the order a launch takes them (reverse != 0: the order
+ * of the alternate launches, which lay the bands out from the last row up): band q covers
+ * rows [out[3q], out[3q+1]) in out[3q+2] blocks of 7 rows.  Fills at most cap bands and
+ * returns the band count (-1: bad arguments).  Host-only; no device work. */
+int fg2_tile_bands(int n1, int nb, int tail, int reverse, int *out, int cap);
 /* Times reps steps of each tiling candidate (tile height 1..8 blocks x occupancy cap: all
- * that fit, 4, 8 or 12 warps per SM) on the simulation's own state with dt = 0 (the state
+ * that fit, 4, 8 or 12 warps per SM x tail bands 0, 1, 3) on the simulation's own state with dt = 0 (the state
  * is left bitwise unchanged; 16-bit storage is kept aside and put back) and keeps the
  * fastest; best_ms (may be NULL) receives its time per step.  A grid whose step takes under
  * 0.05 ms with the default tiling is bound by launch latency and keeps the default.  The

@@ -31,8 +31,33 @@ def test_autotune_leaves_the_state_and_the_results_unchanged(storage, n1, n2, cu
         before = a.download()
         ms = a.autotune(reps=2)
         assert ms > 0
-        nb, ctas = a.tiling()
-        assert 1 <= nb <= 8 and ctas >= 0
+        nb, ctas, tail = a.tiling()
+        assert 1 <= nb <= 8 and ctas >= 0 and tail in (0, 1, 3)
         assert np.array_equal(a.download(), before)
         # the tuned tiling and the default one give bitwise the same steps
         assert np.array_equal(steps(a, 3, dt), steps(b, 3, dt))
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("n1,n2,walls", [(300, 260, False), (1000, 130, True), (64, 200, False)])
+def test_tail_bands_give_the_default_results_bitwise(storage, n1, n2, walls, cuda):
+    """Every tile height with and without one-block tail bands, in both launch directions (a
+    step has three launches, so consecutive steps start in alternate directions), computes
+    every row once and gives bitwise the default tiling's steps."""
+    x = fg2_b200.setup_evaluate("kh", n1, n2, seed=4)[0].astype(np.float32)
+    dt = 2e-5
+
+    def run(tiling):
+        with fg2_b200.Sim(n1, n2, storage=storage) as s:
+            if walls:
+                s.set_bcond(0, 0)
+            s.config()
+            s.upload(x)
+            if tiling:
+                s.set_tiling(*tiling)
+                assert s.tiling() == tiling
+            return steps(s, 4, dt)
+
+    ref = run(None)
+    for tiling in [(1, 0, 0), (3, 0, 1), (3, 1, 3), (5, 0, 2), (8, 0, 1), (8, 2, 0)]:
+        assert np.array_equal(run(tiling), ref), tiling
