@@ -480,7 +480,10 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
                          "ctas_per_sm": ctas, "autotune_step_ms": tune_ms},
               "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ALG_ISOT,
                            "achieved": value * B_ALG_ISOT, "peak": peak, "unit": "GB/s",
-                           "frac": value * B_ALG_ISOT / peak},
+                           "frac": value * B_ALG_ISOT / peak,
+                           "traffic": profiled_traffic("substage_batch_isot_c4"),
+                           "traffic_unit": "DRAM bytes per step (three launches), one ncu capture",
+                           "algorithmic_bytes_per_step": B_ALG_ISOT * total_cells},
               "gpu_launches_per_step": 4}
     if world > 1:
         result.update(n_gpus=world, scaling="strong", sharding="members by cell count, no exchange",
@@ -502,6 +505,10 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
         s.set_time(0.0)
         s.advance(4, 0.0, graph=True)
         sims.append(s)
+    # one untimed pass over every simulation: the first pass's host-side enqueue of 512
+    # graphs runs up to 1.3x slower than later ones
+    for s in sims:
+        s.advance(k_alone, 0.0, graph=True)
     torch.cuda.synchronize()
     e0.record(alone_stream)
     for s in sims:
