@@ -148,6 +148,25 @@ class ClockSampler:
 
 
 # ---- CPU arithmetic of the reference ------------------------------------------------------
+def host_cpu():
+    """The host's logical CPU count and model name (/proc/cpuinfo), recorded beside CPU rates."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+def flop_model(nvar, eqns_flop):
+    """The reference's flop model per cell-step, 3 (eqns_flop + 2 NVAR) (src/config.cpp:33)."""
+    return 3 * (eqns_flop + 2 * nvar)
+
+
 def cpu_sample(state, rows, steps, dt):
     """Time `steps` RK3 steps of the reference's CPU arithmetic on a periodic 4096-wide strip
     of `rows` rows cut from the workload's state.  Returns (Gcell-steps/s, kind, cores)."""
@@ -316,7 +335,8 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
         "config": config_of(args.storage, world),
         "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
-                         "sample": f"each step: {per} RK3 step(s) on a periodic {rows}x{N2} strip of the 4096^2 state"},
+                         "sample": f"each step: {per} RK3 step(s) on a periodic {rows}x{N2} strip of the 4096^2 state",
+                         "ns_per_cell_step": 1.0 / value, "host": host_cpu()},
         "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ns_per_cell_step": 1.0 / value,
     }
@@ -433,6 +453,7 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
     import torch
     import fg2_b200
     all_sizes = batch_sizes()
+    isot_fpc = flop_model(3, fg2_b200.load_library("hydro-isot").fg2_eqns_flop())  # 660
     mine = fg2_b200.shard_members(all_sizes, world)[rank]
     sizes = [all_sizes[k] for k in mine]
     two_pi = 2 * np.pi
@@ -484,6 +505,7 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
                            "traffic": profiled_traffic("substage_batch_isot_c4"),
                            "traffic_unit": "DRAM bytes per step (three launches), one ncu capture",
                            "algorithmic_bytes_per_step": B_ALG_ISOT * total_cells},
+              "flops_ref_model": {"gflops": value * isot_fpc, "flop_per_cell_step": isot_fpc},
               "gpu_launches_per_step": 4}
     if world > 1:
         result.update(n_gpus=world, scaling="strong", sharding="members by cell count, no exchange",
@@ -846,6 +868,7 @@ def run_fused(args):
 
     sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=args.storage)
     b_alg = B_ALG_F16 if args.storage in ("f16", "bf16") else B_ALG  # 160 B FP32, 112 B 16-bit
+    fpc = flop_model(NVAR, sim.lib.fg2_eqns_flop())  # 891 for hydro
     sim.config()
     state = initial_state()
     sim.upload(state)
@@ -936,7 +959,8 @@ def run_fused(args):
         rows, per = calibrated_sample(state, CPU_DT, 20.0, 2)
         rate, kind, cores, el = cpu_sample(state, rows, per, CPU_DT)
         cpu = {"value": rate, "unit": "Gcell-steps/s", "cores": cores, "kind": kind,
-               "sample": f"{per} RK3 steps on a periodic {rows}x{N2} strip of the 4096^2 state ({el:.1f} s)"}
+               "sample": f"{per} RK3 steps on a periodic {rows}x{N2} strip of the 4096^2 state ({el:.1f} s)",
+               "ns_per_cell_step": 1.0 / rate, "host": host_cpu()}
 
     if rank == 0:
         line = {
@@ -950,7 +974,11 @@ def run_fused(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "frac_nominal_8tbs": achieved / 8000.0,
-                         "bytes_per_cell_step": b_alg, "stage_ms": stage_ms},
+                         "bytes_per_cell_step": b_alg, "stage_ms": stage_ms,
+                         "dram_gbs_from_traffic": traffic / (sum(stage_ms) / 1e3) / 1e9 if traffic else None},
+            "flops_ref_model": {"gflops": value * fpc, "flop_per_cell_step": fpc,
+                                "what": "the reference's model 3 (eqns_flop + 2 NVAR) per cell-step (src/config.cpp:33); "
+                                        "a secondary figure: the path is HBM-bound"},
             "step_hbm_frac": value / world * b_alg / peak,
             "tiling": {"blocks_of_7_rows": tiling[0], "ctas_per_sm": tiling[1], "tail_bands": tiling[2],
                        "strip_columns": 128,
