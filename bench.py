@@ -598,17 +598,22 @@ DISK_FLOP = 3 * (733 + 2 * 6)  # the reference's flop model per cell-step (src/c
 DISK_B_ALG = 10 * 6 * 4  # 240 B per cell-step (six FP32 fields)
 
 
-def run_disk_leg(steps, warmup, device):
+def run_disk_leg(steps, warmup, device, tiling=None):
     """The disk scheme (six fields, log-r / theta grid, 733-flop right-hand side) at
     2048 x 2048 on the smooth torus-like state, FP32, fixed dt, steps replayed from the
-    two-step CUDA graph.  Compute-heavy: reported against the reference's flop model and
-    against HBM."""
+    two-step CUDA graph, tiling autotuned (or fixed by `tiling`).  Compute-heavy: reported
+    against the reference's flop model and against HBM."""
     import torch
     import fg2_b200
     peak, _ = peaks()
     with fg2_b200.Sim(DISK_N, DISK_N, scheme="disk") as sim:
         sim.config()
         sim.init("smooth", seed=3)
+        if tiling:
+            sim.set_tiling(*tiling)
+        else:
+            sim.autotune(reps=3)
+        tiled = sim.tiling()
         stream = torch.cuda.ExternalStream(sim.stream, device=device)
         sim.set_time(0.0)
         sim.advance(max(warmup, 3), DISK_DT, graph=True)
@@ -630,9 +635,13 @@ def run_disk_leg(steps, warmup, device):
     return {"workload": f"disk {DISK_N}x{DISK_N} smooth torus-like state (seed 3), FP32, fixed dt {DISK_DT:g}, walls",
             "value": value, "unit": "Gcell-steps/s", "steps": steps, "ms_per_step": ms / steps, "status": status,
             "gflops_ref_model": value * DISK_FLOP, "flop_per_cell_step": DISK_FLOP,
+            "tiling": {"blocks_of_7_rows": tiled[0], "ctas_per_sm": tiled[1], "tail_bands": tiled[2],
+                       "how": "fixed" if tiling else "fg2_sim_autotune"},
             "accuracy_vs_f64": dict(acc, grid=[nd, nd]),
             "roofline": {"bound": "compute", "bytes_per_cell_step": DISK_B_ALG, "hbm_achieved": value * DISK_B_ALG,
-                         "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak}}
+                         "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak,
+                         "traffic": profiled_traffic("substage_disk_2048"),
+                         "traffic_unit": "DRAM bytes per step (three launches), one ncu capture"}}
 
 
 def f16_numbers(x):
@@ -856,9 +865,10 @@ def run_fused(args):
         torch.cuda.set_device(0)
         print(json.dumps(run_precision_leg(8192, 500, torch.device("cuda", 0))), flush=True)
         return
-    if args.only_disk:  # the disk-scheme leg alone (profiling)
+    if args.only_disk:  # the disk-scheme leg alone (profiling: --tiling fixes its tiling)
         torch.cuda.set_device(0)
-        print(json.dumps(run_disk_leg(args.steps, args.warmup, torch.device("cuda", 0))), flush=True)
+        tiling = tuple(int(x) for x in args.tiling.split(",")) if args.tiling else None
+        print(json.dumps(run_disk_leg(args.steps, args.warmup, torch.device("cuda", 0), tiling)), flush=True)
         return
 
     rank, local, world = dist_env()
