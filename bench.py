@@ -640,7 +640,7 @@ def run_disk_leg(steps, warmup, device, tiling=None):
             "accuracy_vs_f64": dict(acc, grid=[nd, nd]),
             "roofline": {"bound": "compute", "bytes_per_cell_step": DISK_B_ALG, "hbm_achieved": value * DISK_B_ALG,
                          "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak,
-                         "traffic": profiled_traffic("substage_disk_2048"),
+                         "traffic": profiled_traffic("substage_disk_f32_2048"),
                          "traffic_unit": "DRAM bytes per step (three launches), one ncu capture"}}
 
 
