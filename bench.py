@@ -101,15 +101,16 @@ CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.ac
 
 
 class ClockSampler:
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=200):
         self.index = index
+        self.interval_ms = interval_ms
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={CLOCK_QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
             time.sleep(0.3)
         except OSError:
@@ -621,10 +622,11 @@ def run_disk_leg(steps, warmup, device, tiling=None):
             raise RuntimeError("disk warm-up produced a bad status")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        e0.record(stream)
-        sim.advance(steps, DISK_DT, graph=True)
-        e1.record(stream)
-        e1.synchronize()
+        with ClockSampler(device.index or 0, 50) as clk:
+            e0.record(stream)
+            sim.advance(steps, DISK_DT, graph=True)
+            e1.record(stream)
+            e1.synchronize()
         ms = e0.elapsed_time(e1)
         status = sim.sync()
     cells = DISK_N * DISK_N
@@ -637,6 +639,7 @@ def run_disk_leg(steps, warmup, device, tiling=None):
             "gflops_ref_model": value * DISK_FLOP, "flop_per_cell_step": DISK_FLOP,
             "tiling": {"blocks_of_7_rows": tiled[0], "ctas_per_sm": tiled[1], "tail_bands": tiled[2],
                        "how": "fixed" if tiling else "fg2_sim_autotune"},
+            "clocks": clk.summary(),
             "accuracy_vs_f64": dict(acc, grid=[nd, nd]),
             "roofline": {"bound": "compute", "bytes_per_cell_step": DISK_B_ALG, "hbm_achieved": value * DISK_B_ALG,
                          "hbm_peak": peak, "unit": "GB/s", "hbm_frac": value * DISK_B_ALG / peak,
