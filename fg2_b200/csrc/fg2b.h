@@ -132,10 +132,11 @@ struct DevCode {
   void *r;               // rounding residual of the state (16-bit numbers, layout of v)
 };
 
-// ---- arithmetic on a scalar or on a pair of cells ------------------------------------------
-// The fused kernel evaluates two cells per thread; for FP32 the pair is a float2 and every
-// operation is one packed sm_100 instruction (add/mul/fma .f32x2), for FP64 a double2
-// evaluated component-wise.  Scheme code is written once against these helpers.
+// ---- arithmetic on a scalar or on a pair ----------------------------------------------------
+// The fused kernel's stencil works on pairs of fields of a cell: for FP32 the pair is a float2
+// and every operation is one packed sm_100 instruction (add/mul/fma .f32x2), for FP64 a
+// double2 evaluated component-wise.  Scheme code (eqns, the CFL rate) is written against the
+// same helpers and evaluated per cell on scalars.
 template <class C>
 struct Scalar {
   using type = C;

@@ -1,7 +1,7 @@
 // schemes/hydro-isot/eqns.cuh -- right-hand side of the isothermal equations in
 // log-density form with shear/bulk viscosity, optional density diffusion and optional
 // Kolmogorov forcing.  Physics and runtime keys follow src/hydro-isot/eqns.cuh:19-87; the
-// derivatives arrive precomputed in a Cell; C is a scalar or a pair of cells.
+// derivatives arrive precomputed in a Cell; C is the compute type (float or double).
 #pragma once
 
 #include <cmath>
@@ -44,7 +44,7 @@ FG2_HD Geom<C> column_geom(int j, C delta2)
   return Geom<C>{};
 }
 
-// dq/dt at one cell (or cell pair in the same row i; Kolmogorov forcing varies with i).
+// dq/dt at one cell (Kolmogorov forcing varies with its row i).
 template <unsigned M2, class C>
 FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2,
                  const Geom<C> &)

@@ -1,8 +1,8 @@
 // schemes/hydro/eqns.cuh -- right-hand side of the ideal-gas equations in log-primitive
 // form, with shear/bulk viscosity, viscous heating, thermal conduction and optional
 // density diffusion.  Physics and runtime keys follow src/hydro/eqns.cuh:19-92.  The
-// derivatives arrive precomputed in a Cell; C is a scalar or a pair of cells (two cells per
-// thread, packed FP32x2 arithmetic), so every product-sum is written as an explicit fmac.
+// derivatives arrive precomputed in a Cell; C is the compute type (float or double), and
+// every product-sum is written as an explicit fmac.
 #pragma once
 
 #include <cmath>
@@ -52,7 +52,7 @@ FG2_HD Geom<C> column_geom(int j, C delta2)
   return Geom<C>{};
 }
 
-// dq/dt at one cell (or cell pair).  M2 is the set of fields whose D11/D22 the caller
+// dq/dt at one cell.  M2 is the set of fields whose D11/D22 the caller
 // evaluated; the others read as zero.  i, j and the spacings are unused by this scheme.
 template <unsigned M2, class C>
 FG2_HD void eqns(const fg2::Cell<C, NVAR> &c, const fg2::Para<C> &p, int i, int j, C r[NVAR], C delta1, C delta2,
