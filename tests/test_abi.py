@@ -84,6 +84,15 @@ def test_bad_sizes_rejected_before_any_device_call():
     assert not lib.fg2_sim_create(64, 64, 7, None)
 
 
+def test_tiling_entry_points_reject_null_handles_and_bad_values():
+    lib = fg2_b200.load_library("hydro")
+    t = ctypes.c_int(-7)
+    assert lib.fg2_sim_set_tail(None, 1) != 0
+    assert lib.fg2_sim_get_tail(None, ctypes.byref(t)) != 0 and t.value == -7
+    assert lib.fg2_sim_set_tiling(None, 3) != 0
+    assert lib.fg2_sim_set_occupancy(None, 1) != 0
+
+
 # ---- host-side initial conditions -------------------------------------------------------
 M64 = (1 << 64) - 1
 

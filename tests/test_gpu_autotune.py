@@ -61,3 +61,13 @@ def test_tail_bands_give_the_default_results_bitwise(storage, n1, n2, walls, cud
     ref = run(None)
     for tiling in [(1, 0, 0), (3, 0, 1), (3, 1, 3), (5, 0, 2), (8, 0, 1), (8, 2, 0)]:
         assert np.array_equal(run(tiling), ref), tiling
+
+
+def test_bad_tail_band_counts_are_refused(cuda):
+    with fg2_b200.Sim(64, 64) as s:
+        s.config()
+        for bad in (-1, 65):
+            with pytest.raises(fg2_b200.FG2Error):
+                s.set_tiling(3, 0, bad)
+        s.set_tiling(3, 0, 2)
+        assert s.tiling() == (3, 0, 2)
