@@ -550,11 +550,12 @@ def run_batch_leg(steps, warmup, device, tiling=None, one_at_a_time=True, rank=0
 
 
 # ---- the 16-bit deviation-storage path (secondary results) ----------------------------------
-# 16-bit storage: u, v and the rounding residual r, 2 B per value.  Stage 0 reads u, r and
-# writes u', v, r; stage 1 reads u, v, r and writes u', v (its residual folded into v); stage 2
-# reads u, v and writes u', r: 14 array passes, 112 B per cell-step for hydro (80 B of them the
-# plain RK3 traffic of u and v, 32 B the compensation)
-B_ALG_F16 = 14 * NVAR * 2
+# 16-bit storage: u, v and the rounding residual r of u, 2 B per value.  Every stage reads u
+# with its residual r (the stencil reads the compensated state) and writes u' with its
+# residual; stage 0 also writes v, stage 1 reads and writes v, stage 2 reads v: 16 array
+# passes, 128 B per cell-step for hydro (80 B of them the plain RK3 traffic of u and v, 48 B
+# the compensation)
+B_ALG_F16 = 16 * NVAR * 2
 
 
 def run_mixed_leg(state, steps, warmup, device, plain_value):

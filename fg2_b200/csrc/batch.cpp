@@ -99,7 +99,7 @@ int ensure_batch_descs(fg2_batch *b, bool device_dt)
     for (int set = 0; set < 2; ++set) {
       const int in = set == 0 ? m->cur : 1 - m->cur;
       if (make_grid_desc(&b->desc_host[(size_t)set * b->count + r], m->u[in], m->u[1 - in], m->v, m->L, m->storage,
-                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0, dev_code(m),
+                         m->p1, m->p2, m->delta1, m->delta2, dt, &b->status[k], tile0, dev_code_at(m, in),
                          b->strip) != CUDA_SUCCESS)
         return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed for batch member %d", k);
     }
@@ -142,7 +142,6 @@ int enqueue_batch_step(fg2_batch *b, double dt, bool device_dt, double t_end, in
     a.strip = b->strip;
     a.reverse = b->reverse;
     b->reverse ^= 1;
-    a.comp_bg = k == 1 ? RK_BETA[2] * RK_GAMMA[2] : 0.0;  // 16-bit stage 1 folds its residual into v
     const int kind = k == 0 ? STAGE_FIRST : k == 1 ? STAGE_MID : STAGE_LAST;
     CK(launch_substage(b->storage, kind, device_dt && k == 2, true, b->desc + (size_t)set * b->count, b->count,
                        b->ntiles, a, b->queue, b->stream));
@@ -269,13 +268,13 @@ fg2_batch *fg2_batch_create(int count, const int *n1, const int *n2, int storage
   char *p = (char *)b->arena;
   const int na = arrays_per_sim(storage);
   for (int k = 0; k < count; ++k) {
-    void *r = na > 3 ? p + 3 * bytes[k] : nullptr;  // 16-bit storage: the rounding residual
-    if (r && cudaMemsetAsync(r, 0, bytes[k], b->stream) != cudaSuccess) {
+    void *r = na > 3 ? p + 3 * bytes[k] : nullptr;  // 16-bit storage: the residuals of u[0], u[1]
+    if (r && cudaMemsetAsync(r, 0, 2 * bytes[k], b->stream) != cudaSuccess) {
       fail(FG2_ERR_ALLOC, "initial fill of the batch failed");
       return nullptr;
     }
-    fg2_sim *m = sim_create_in(n1[k], n2[k], storage, b->stream, p, p + bytes[k], p + 2 * bytes[k], r, &b->status[k],
-                               &b->status_host[k]);
+    fg2_sim *m = sim_create_in(n1[k], n2[k], storage, b->stream, p, p + bytes[k], p + 2 * bytes[k], r,
+                               r ? p + 4 * bytes[k] : nullptr, &b->status[k], &b->status_host[k]);
     if (!m) return nullptr;
     b->members.push_back(m);
     p += na * bytes[k];

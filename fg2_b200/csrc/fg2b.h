@@ -129,7 +129,8 @@ struct DevCode {
   const float4 *scale;   // per tile, row-major over (n1 / 64, n2 / 64) tiles: s of each field
   const float4 *inv;     // per tile: 1 / s
   int tiles2;            // tiles along axis 2
-  void *r;               // rounding residual of the state (16-bit numbers, layout of v)
+  void *r;               // rounding residual of the state read (16-bit numbers, layout of u)
+  void *r_out;           // rounding residual of the state a substage writes
 };
 
 // ---- arithmetic on a scalar or on a pair ----------------------------------------------------

@@ -95,7 +95,6 @@ struct KParams {
   int strip;             // strip width (columns per tile, threads per CTA)
   int reverse;           // tiles last first
   unsigned wait_test_bytes;  // extra bytes every chunk expects (timeout-path tests; 0 otherwise)
-  double comp_bg;        // beta * gamma of the next stage (16-bit residual carry), or 0
 };
 
 template <class T>
@@ -152,7 +151,6 @@ static KParams<T> make_params(const StageArgs &a, bool scaled)
   kp.nb = a.nb > 0 ? a.nb : TILE_BLOCKS_DEFAULT;
   kp.tail = a.tail > 0 ? a.tail : 0;
   kp.strip = strip_width(a.strip);
-  kp.comp_bg = a.comp_bg;
   kp.reverse = a.reverse;
   kp.wait_test_bytes = a.wait_test_bytes;
   return kp;
@@ -275,8 +273,8 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   const int G = group_cells(storage), vbw = (sw + GL % G + G - 1) / G * G;
   r = encode_map(&d->tm_v, v, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
-  if (dev && dev->r) {
-    r = encode_map(&d->tm_r, dev->r, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+  if (dev && dev->r) {  // the input's rounding residual, in boxes like u's (halo included)
+    r = encode_map(&d->tm_r, dev->r, L, storage, sw + 2 * GL, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
     if (r != CUDA_SUCCESS) return r;
   } else {
     d->tm_r = d->tm_v;  // never read: only 16-bit stages load r
@@ -298,7 +296,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   d->delta1 = delta1;
   d->delta2 = delta2;
   if (dev) d->dev = *dev;
-  else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0, nullptr};
+  else d->dev = DevCode{{0.f, 0.f, 0.f, 0.f}, nullptr, nullptr, 0, nullptr, nullptr};
   return CUDA_SUCCESS;
 }
 
@@ -331,7 +329,7 @@ template <class S, unsigned M2, bool RV, bool WV, bool WU, bool CF, bool SC, int
 static cudaError_t run_substage_w(const GridDesc *grids, int ngrids, int ntiles, const KParams<typename Store<S>::C> &kp,
                                   int max_ctas, int *queue, cudaStream_t s)
 {
-  using G = sub::Geo<S, RV, Store<S>::DEV && WU && WV, W>;  // 16-bit stages 0 and 1 also load r
+  using G = sub::Geo<S, RV, Store<S>::DEV, W>;  // 16-bit stages also load the residual box
   auto kern = sub::substage_kernel<S, M2, RV, WV, WU, CF, SC, W>;
   static int ctas_per_sm = 0, sms = 0;
   if (!ctas_per_sm) {

@@ -30,8 +30,6 @@ struct StageArgs {
   int max_ctas = 0;     // CTAs per SM of the persistent grid (0: as many as fit)
   int strip = 0;        // strip width: 64 or 128 columns per tile (0: 128); one thread per
                         // column, so 2 or 4 warps per CTA; the descriptors must match it
-  double comp_bg = 0;   // 16-bit storage, stage 1: beta * gamma of stage 2, which reads the
-                        // stage's rounding residual folded into v (0: other stages)
   int reverse = 0;      // take the tiles last first (alternated from launch to launch, so a
                         // stage starts on the tiles the previous one wrote last, still in L2)
   unsigned wait_test_bytes = 0;  // tests of the timeout path: every chunk expects this many

@@ -115,7 +115,6 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   a.p1 = s->p1;
   a.p2 = s->p2;
   a.status = s->status;
-  a.comp_bg = k == 1 ? RK_BETA[2] * RK_GAMMA[2] : 0.0;  // 16-bit stage 1 folds its residual into v
   a.wait_test_bytes = s->wait_test_bytes;
   a.nb = tile_height(s);
   a.tail = s->tail;
@@ -123,7 +122,16 @@ StageArgs stage_args(fg2_sim *s, int k, double dt, const double *dt_dev)
   return a;
 }
 
-const DevCode *dev_code(const fg2_sim *s) { return s->dev_storage ? &s->dev : nullptr; }
+const DevCode *dev_code_at(const fg2_sim *s, int k)
+{
+  if (!s->dev_storage) return nullptr;
+  s->devk[k] = s->dev;
+  s->devk[k].r = s->r[k];
+  s->devk[k].r_out = s->r[1 - k];
+  return &s->devk[k];
+}
+
+const DevCode *dev_code(const fg2_sim *s) { return dev_code_at(s, s->cur); }
 
 // The two ping-pong descriptors (boundaries and Delta as configured); uploaded before any
 // capture, since every path that launches a substage calls this first.
@@ -132,7 +140,7 @@ int ensure_descs(fg2_sim *s)
   if (s->desc_valid) return FG2_OK;
   for (int k = 0; k < 2; ++k)
     if (make_grid_desc(&s->desc_host[k], s->u[k], s->u[1 - k], s->v, s->L, s->storage, s->p1, s->p2, s->delta1,
-                       s->delta2, nullptr, s->status, 0, dev_code(s)) != CUDA_SUCCESS)
+                       s->delta2, nullptr, s->status, 0, dev_code_at(s, k)) != CUDA_SUCCESS)
       return fail(FG2_ERR_TMA, "cuTensorMapEncodeTiled failed");
   CK(cudaMemcpyAsync(s->desc, s->desc_host, 2 * sizeof(GridDesc), cudaMemcpyHostToDevice, s->stream));
   CK(cudaStreamSynchronize(s->stream));
@@ -171,6 +179,8 @@ int ensure_config(fg2_sim *s)
 int do_bcond(fg2_sim *s)
 {
   CK(launch_bcond(s->storage, s->u[s->cur], s->L, s->p1, s->p2, s->stream));
+  // 16-bit storage: the residual's ghost cells image the same cells (the stencil reads T = S - e)
+  if (s->dev_storage) CK(launch_bcond(s->storage, s->r[s->cur], s->L, s->p1, s->p2, s->stream));
   s->ghosts_valid = true;
   return FG2_OK;
 }
@@ -282,15 +292,17 @@ int transfer_dev(fg2_sim *s, void *dev_array, void *host, bool to_device)
   float *tmp = nullptr;
   CK(cudaMalloc(&tmp, n * sizeof(float)));
   std::unique_ptr<float, cudaError_t (*)(void *)> hold(tmp, cudaFree);
+  if (to_device && is_u) {  // an upload of the state sets the background and scales first
+    int rc = set_codes(s, (const float *)host);
+    if (rc) return rc;
+  }
+  // the codes of the parity transferred, with its residual array
+  const DevCode *dc = is_u ? dev_code_at(s, dev_array == s->u[0] ? 0 : 1) : nullptr;
   if (to_device) {
-    if (is_u) {
-      int rc = set_codes(s, (const float *)host);
-      if (rc) return rc;
-    }
     CK(cudaMemcpyAsync(tmp, host, n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CK(launch_encode(s->storage, dev_array, tmp, s->L, is_u ? &s->dev : nullptr, s->stream));
+    CK(launch_encode(s->storage, dev_array, tmp, s->L, dc, s->stream));
   } else {
-    CK(launch_decode(s->storage, tmp, dev_array, s->L, is_u ? &s->dev : nullptr, s->stream));
+    CK(launch_decode(s->storage, tmp, dev_array, s->L, dc, s->stream));
     CK(cudaMemcpyAsync(host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   }
   CK(cudaStreamSynchronize(s->stream));
@@ -446,8 +458,8 @@ fg2_sim *new_handle(int n1, int n2, int storage, cudaStream_t stream, bool own_a
 
 }  // namespace
 
-fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r,
-                       Status *status, Status *status_host)
+fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r0,
+                       void *r1, Status *status, Status *status_host)
 {
   fg2_sim *s = new_handle(n1, n2, storage, stream, false);
   if (!s) return nullptr;
@@ -457,13 +469,13 @@ fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u
   s->status = status;
   s->status_host = status_host;
   if (s->dev_storage) {
-    s->r = r;
-    s->dev.r = r;
+    s->r[0] = r0;
+    s->r[1] = r1;
   }
   return s;
 }
 
-int arrays_per_sim(int storage) { return storage == ST_F16 || storage == ST_BF16 ? 4 : 3; }
+int arrays_per_sim(int storage) { return storage == ST_F16 || storage == ST_BF16 ? 5 : 3; }
 
 }  // namespace rt
 }  // namespace fg2
@@ -477,11 +489,11 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (!s) return nullptr;
   const size_t bytes = array_elems(s.get()) * elem_size(storage);
   if (cudaMalloc(&s->u[0], bytes) != cudaSuccess || cudaMalloc(&s->u[1], bytes) != cudaSuccess ||
-      cudaMalloc(&s->v, bytes) != cudaSuccess || (s->dev_storage && cudaMalloc(&s->r, bytes) != cudaSuccess)) {
+      cudaMalloc(&s->v, bytes) != cudaSuccess ||
+      (s->dev_storage && (cudaMalloc(&s->r[0], bytes) != cudaSuccess || cudaMalloc(&s->r[1], bytes) != cudaSuccess))) {
     fail(FG2_ERR_ALLOC, "device allocation of the state failed");
     return nullptr;
   }
-  s->dev.r = s->r;  // null unless 16-bit storage
   if (cudaMalloc(&s->status, sizeof(Status)) != cudaSuccess ||
       cudaMallocHost(&s->status_host, sizeof(Status)) != cudaSuccess) {
     fail(FG2_ERR_ALLOC, "status allocation failed");
@@ -492,7 +504,8 @@ fg2_sim *fg2_sim_create(int n1, int n2, int storage, void *stream)
   if (launch_fill(storage, s->u[0], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->u[1], array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
       launch_fill(storage, s->v, array_elems(s.get()), lowest, s->stream) != cudaSuccess ||
-      (s->r && cudaMemsetAsync(s->r, 0, bytes, s->stream) != cudaSuccess) ||
+      (s->r[0] && cudaMemsetAsync(s->r[0], 0, bytes, s->stream) != cudaSuccess) ||
+      (s->r[1] && cudaMemsetAsync(s->r[1], 0, bytes, s->stream) != cudaSuccess) ||
       cudaMemsetAsync(s->status, 0, sizeof(Status), s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess) {
     fail(FG2_ERR_ALLOC, "initial fill failed");
@@ -510,7 +523,8 @@ void fg2_sim_destroy(fg2_sim *s)
     cudaFree(s->u[0]);
     cudaFree(s->u[1]);
     cudaFree(s->v);
-    cudaFree(s->r);
+    cudaFree(s->r[0]);
+    cudaFree(s->r[1]);
     cudaFree(s->status);
     cudaFreeHost(s->status_host);
   }
@@ -604,7 +618,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   if (s->dev_storage) {
     CK(cudaMalloc(&keep, 2 * bytes));
     CK(cudaMemcpyAsync(keep, s->u[s->cur], bytes, cudaMemcpyDeviceToDevice, s->stream));
-    CK(cudaMemcpyAsync((char *)keep + bytes, s->r, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync((char *)keep + bytes, s->r[keep_cur], bytes, cudaMemcpyDeviceToDevice, s->stream));
   }
   std::unique_ptr<void, cudaError_t (*)(void *)> hold(keep, cudaFree);
   cudaEvent_t e0, e1;
@@ -650,7 +664,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
   cudaEventDestroy(e1);
   if (keep) {
     CK(cudaMemcpyAsync(s->u[keep_cur], keep, bytes, cudaMemcpyDeviceToDevice, s->stream));
-    CK(cudaMemcpyAsync(s->r, (char *)keep + bytes, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->r[keep_cur], (char *)keep + bytes, bytes, cudaMemcpyDeviceToDevice, s->stream));
   }
   CK(cudaStreamSynchronize(s->stream));
   // every stage of dt = 0 copied the state bitwise into the array it wrote, ghost images

@@ -61,8 +61,9 @@ struct fg2_sim {
   bool dev_storage = false;
   int tiles1 = 0, tiles2 = 0;
   float4 *scale_dev = nullptr, *inv_dev = nullptr;
-  void *r = nullptr;  // rounding residual of the state (16-bit numbers, layout of v)
-  fg2::DevCode dev{};
+  void *r[2] = {nullptr, nullptr};  // rounding residual of u[0] and of u[1] (16-bit numbers, layout of u)
+  fg2::DevCode dev{};                // background and scales (shared by both parities)
+  mutable fg2::DevCode devk[2]{};    // dev with the residual arrays of parity k: read r[k], write r[1 - k]
 };
 
 namespace fg2 {
@@ -86,15 +87,17 @@ int do_euler(fg2_sim *s, double dt);
 bool euler_active(const fg2_sim *s);
 double diffusive_dt(const fg2_sim *s);
 int read_status(fg2_sim *s);
-// The handle's deviation codes for kernels that decode the state (null: plain storage).
+// The handle's deviation codes for kernels that decode the state u[cur] (null: plain storage),
+// and for parity k: the residual of u[k] read, that of u[1 - k] written.
 const fg2::DevCode *dev_code(const fg2_sim *s);
+const fg2::DevCode *dev_code_at(const fg2_sim *s, int k);
 void drop_graph(fg2_sim *s);
 // A handle over caller-owned device memory: arrays u0, u1, v (and, for 16-bit storage, the
-// residual r, zero-filled) of the handle's layout and one status block (device) with its
-// pinned host mirror; the handle frees none of them.
-fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r,
-                       Status *status, Status *status_host);
-// Arrays per simulation in device memory: u[0], u[1], v, and r for 16-bit storage.
+// residual arrays r0, r1 of u0 and u1, zero-filled) of the handle's layout and one status
+// block (device) with its pinned host mirror; the handle frees none of them.
+fg2_sim *sim_create_in(int n1, int n2, int storage, cudaStream_t stream, void *u0, void *u1, void *v, void *r0,
+                       void *r1, Status *status, Status *status_host);
+// Arrays per simulation in device memory: u[0], u[1], v, and r[0], r[1] for 16-bit storage.
 int arrays_per_sim(int storage);
 
 }  // namespace rt

@@ -101,7 +101,8 @@ __host__ __device__ constexpr int group_of(int elem)
 }
 
 // Shared memory of one CTA: NSLOT slots of [u box | v box | r box] (the v box only when the
-// stage reads v, the r box only when it reads the rounding residual of 16-bit storage), two
+// stage reads v, the r box -- the rounding residual of a 16-bit u box, the same cells -- only
+// with 16-bit storage), two
 // FP32 copies of a landed u box (deviation storage: chunk n is stenciled from one while chunk
 // n + 1 is decoded into the other), then the mbarriers and the producer's bookkeeping.  The
 // v and r boxes start VOFF cells left of the strip when a cell group is wider than the 4
@@ -119,8 +120,9 @@ struct Geo {
   static constexpr uint32_t V_OFF = (U_BYTES + 127) / 128 * 128;  // TMA destinations on 128 B
   static constexpr uint32_t V_BYTES = (uint32_t)(VBW * CH * CB);
   static constexpr uint32_t V_AL = (V_BYTES + 127) / 128 * 128;
+  static constexpr uint32_t U_AL = (U_BYTES + 127) / 128 * 128;
   static constexpr uint32_t R_OFF = V_OFF + (RV ? V_AL : 0);
-  static constexpr uint32_t SLOT = R_OFF + (RR ? V_AL : 0);
+  static constexpr uint32_t SLOT = R_OFF + (RR ? U_AL : 0);
   static constexpr size_t DEC_OFF = (size_t)NSLOT * SLOT;
   static constexpr size_t DEC_ONE = DEV ? ((size_t)BW * CH * NV * sizeof(float) + 127) / 128 * 128 : 0;
   static constexpr size_t DEC_BYTES = 2 * DEC_ONE;
@@ -340,9 +342,8 @@ struct GridRegs {
   T s12, inv1, inv2, delta1, delta2;  // 1/(Delta1 Delta2), CFL factors, Delta1, Delta2
   // deviation storage
   P bg[NP];                    // per-field background
-  P comp;                      // -1 / (beta' gamma' dt) of the next stage (stage 1), or 0
   const float4 *scale, *inv;   // per-tile s and 1/s
-  S *r;                        // rounding residual array
+  S *r;                        // rounding residual of the state the stage writes
   int tiles2;
 };
 
@@ -599,9 +600,8 @@ __device__ __forceinline__ void gather_row(const KParams<T> &a, const GR &gr, co
 template <class S, unsigned M2, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
 __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> &cell,
                                            const typename PairOf<typename Store<S>::C>::type qc[NP],
-                                           const typename PairOf<typename Store<S>::C>::type vr[NP],
-                                           const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j, int iend,
-                                           const float4 &scv, const float4 &ivv,
+                                           const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
+                                           int iend, const float4 &scv, const float4 &ivv,
                                            const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr, bool full,
                                            bool rim, bool &nan, typename Store<S>::C &rate,
                                            const scheme::Geom<typename Store<S>::C> &cg)
@@ -610,9 +610,6 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
   using P = typename PairOf<T>::type;
   using St = Store<S>;
   constexpr bool DEV = St::DEV;
-  constexpr bool RR = DEV && WRITE_U && WRITE_V;                 // stages 0 and 1
-  constexpr bool WR = DEV && WRITE_U && !(READ_V && WRITE_V);    // stages 0 and 2
-  constexpr bool FOLD = DEV && WRITE_U && READ_V && WRITE_V;     // stage 1
   T r[NV];
   const T dl1 = SC ? gr.delta1 : a.ks.delta1, dl2 = SC ? gr.delta2 : a.ks.delta2;
   scheme::eqns<M2>(cell, a.p, i, j, r, dl1, dl2, cg);
@@ -631,35 +628,28 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
   for (int p = 0; p < NP; ++p) {
     vn[p] = PairOf<T>::make(r[2 * p], 2 * p + 1 < NV ? r[2 * p + 1] : T(0));
     if (READ_V) vn[p] = fmac(a.beta2, vr[p], vn[p]);
-    P base = qc[p];
-    if constexpr (RR) base = fmac(rr[p], sc[p] * lit<P>(-1.0 / RESID_SCALE), base);  // T = S - e
-    qp[p] = fmac(gr.gdt, vn[p], base);
+    qp[p] = fmac(gr.gdt, vn[p], qc[p]);
   }
   const long long o = gr.L.at(0, i, j);
   if constexpr (!DEV) {
     if (WRITE_U) store_cell<S>(gr.u_out + o, qp);
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
-  RawCell<S> raw;
+  RawCell<S> raw, rraw;
   if constexpr (DEV) {
     if (WRITE_U) {
-      // encode u' with its tile's 1/s; e' = S' - u' is the rounding residual
-      P h[NP], hs[NP], e[NP];
+      // encode u' with its tile's 1/s; e' = S' - u' is the rounding residual, stored as
+      // e' / s * RESID_SCALE beside it
+      P h[NP], hs[NP], e[NP], ro[NP], unused[NP];
 #pragma unroll
       for (int p = 0; p < NP; ++p) h[p] = (qp[p] - gr.bg[p]) * iv[p];
       encode_cell<S>(gr.u_out + o, h, hs, raw.v);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) e[p] = fmac(sc[p], hs[p], gr.bg[p]) - qp[p];
-      if constexpr (FOLD) {
-#pragma unroll
-        for (int p = 0; p < NP; ++p) vn[p] = fmac(e[p], gr.comp, vn[p]);
+      for (int p = 0; p < NP; ++p) {
+        e[p] = fmac(sc[p], hs[p], gr.bg[p]) - qp[p];
+        ro[p] = e[p] * (iv[p] * lit<P>(RESID_SCALE));
       }
-      if constexpr (WR) {
-        P ro[NP];
-#pragma unroll
-        for (int p = 0; p < NP; ++p) ro[p] = e[p] * (iv[p] * lit<P>(RESID_SCALE));
-        store_cell<S>(gr.r + o, ro);
-      }
+      encode_cell<S>(gr.r + o, ro, unused, rraw.v);
     }
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
@@ -677,7 +667,10 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
         if constexpr (NP == 3) rim_images3<S>(gr.u_out, gr.L, i, j, qp[0], qp[1], qp[2], gr.p1, gr.p2);
         else rim_images<S>(gr.u_out, gr.L, i, j, qp[0], qp[NP - 1], gr.p1, gr.p2);
       }
-      else rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
+      else {
+        rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
+        rim_images_raw<S>(gr.r, gr.L, i, j, rraw, gr.p1, gr.p2);
+      }
     }
     if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2, i, j, dl1, dl2, cg));
   }
@@ -685,9 +678,8 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
 
 // Output row for slot R of a block: the row 3 behind the leading row, slot (R + 4) mod 7.
 template <class S, unsigned M2, int R, bool READ_V, bool WRITE_V, bool WRITE_U, bool CFL, bool SC>
-__device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP],
-                                         const typename PairOf<typename Store<S>::C>::type rr[NP], int i, int j, int iend,
-                                         const float4 &scv, const float4 &ivv,
+__device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>::C>::type vr[NP], int i, int j,
+                                         int iend, const float4 &scv, const float4 &ivv,
                                          const KParams<typename Store<S>::C> &a, const GridRegs<S> &gr,
                                          const Roll<typename Store<S>::C> &s, bool full, bool rim, bool &nan,
                                          typename Store<S>::C &rate, const scheme::Geom<typename Store<S>::C> &cg)
@@ -696,8 +688,8 @@ __device__ __forceinline__ void emit_row(const typename PairOf<typename Store<S>
   Cell<T, NV> cell;
   typename PairOf<T>::type qc[NP];
   gather_row<T, M2, SC, (R + 4) % CH>(a, gr, s, cell, qc);
-  finish_row<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC>(cell, qc, vr, rr, i, j, iend, scv, ivv, a, gr, full, rim, nan,
-                                                       rate, cg);
+  finish_row<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC>(cell, qc, vr, i, j, iend, scv, ivv, a, gr, full, rim, nan, rate,
+                                                       cg);
 }
 
 // Shared state of the chunk issue, read and written by thread 0 only.
@@ -756,8 +748,8 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
   } else {
     const GridDesc &gd = grids[ps->cur.g];
     const int i0 = ps->cur.i0, j0 = ps->cur.j0, c = ps->c, last = ps->cur.nbt;
-    const bool with_v = READ_V && c > 0, with_r = READ_R && c > 0;
-    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + (with_r ? G::V_BYTES : 0u) + extra_bytes);
+    const bool with_v = READ_V && c > 0;
+    mbar_arrive_expect_tx(&full[s], G::U_BYTES + (with_v ? G::V_BYTES : 0u) + (READ_R ? G::U_BYTES : 0u) + extra_bytes);
     // box coordinates (group element, cell group, padded row): rows i0 - 4 + 7c ..,
     // columns j0 - 4 .. (padded column j0)
     tma_load_3d(smem + (size_t)s * G::SLOT, &gd.tm_u, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
@@ -765,10 +757,9 @@ __device__ __forceinline__ void issue_chunk(Producer *ps, unsigned char *smem, u
     if (with_v)
       tma_load_3d(smem + (size_t)s * G::SLOT + G::V_OFF, &gd.tm_v, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
                   i0 + CH * (c - 1) + GT);
-    // the rounding residual of the same cells (16-bit stages 0 and 1)
-    if (with_r)
-      tma_load_3d(smem + (size_t)s * G::SLOT + G::R_OFF, &gd.tm_r, &full[s], 0, (j0 + GL - G::VOFF) / G::G,
-                  i0 + CH * (c - 1) + GT);
+    // 16-bit storage: the rounding residual of the u box's cells
+    if (READ_R)
+      tma_load_3d(smem + (size_t)s * G::SLOT + G::R_OFF, &gd.tm_r, &full[s], 0, j0 / G::G, i0 - 4 + CH * c + GT);
     if (c == last) claim = atomicAdd(&queue[0], 1);  // the next tile's position, used one chunk later
     ps->c = c == last ? 0 : c + 1;
   }
@@ -808,22 +799,23 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
   if constexpr (Store<S>::DEV) {
 #pragma unroll
     for (int p = 0; p < NP; ++p) gr.bg[p] = make_float2(gd.dev.bg[2 * p], gd.dev.bg[2 * p + 1]);
-    gr.comp = lit<P>(a.comp_bg != 0.0 && dt > 0.0 ? -1.0 / (a.comp_bg * dt) : 0.0);
     gr.scale = gd.dev.scale;
     gr.inv = gd.dev.inv;
-    gr.r = reinterpret_cast<S *>(gd.dev.r);
+    gr.r = reinterpret_cast<S *>(gd.dev.r_out);
     gr.tiles2 = gd.dev.tiles2;
   }
 }
 
 // Deviation storage: decodes the landed 7-row u box (padded rows prow0 .., box column 0 =
-// padded column j0) into FP32 cells dec ([row][BOXW][NV]): bg + s h with s of the tile of the
-// interior cell each value images.  Thread t decodes column t of every row and, for t below
+// padded column j0) and its residual box into FP32 cells dec ([row][BOXW][NV]): the state
+// T = bg + s h - s r / RESID_SCALE, s of the tile of the interior cell each value images, so
+// the stencil reads the state with its rounding compensated, not the 16-bit numbers.  Thread t decodes column t of every row and, for t below
 // 7 (BOXW - NT), one cell of the columns beyond the strip, so the work is even across warps.
 // A chunk whose 7 rows lie in one tile row (all but about one chunk in nine) reads each
 // column's scales once.
 template <class S, int BOXW, int NT>
-__device__ __forceinline__ void decode_box(const S *box, float *dec, int tx, int prow0, int j0, const GridRegs<S> &gr)
+__device__ __forceinline__ void decode_box(const S *box, const S *rbox, float *dec, int tx, int prow0, int j0,
+                                           const GridRegs<S> &gr)
 {
   constexpr int EXTRA = BOXW - NT;  // columns beyond one per thread
   const int n1 = gr.L.n1, n2 = gr.L.n2;
@@ -836,10 +828,11 @@ __device__ __forceinline__ void decode_box(const S *box, float *dec, int tx, int
   };
   auto put = [&](int r, int c, float4 sc) {
     const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
-    float2 h[NP];
+    float2 h[NP], e[NP];
     load_cell<S>(box + (r * BOXW + c) * NV, h);
+    load_cell<S>(rbox + (r * BOXW + c) * NV, e);
 #pragma unroll
-    for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p], h[p], gr.bg[p]);
+    for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p] * lit<float2>(-1.0 / RESID_SCALE), e[p], fmac(scp[p], h[p], gr.bg[p]));
     st_cell<float>(dec + (r * BOXW + c) * NV, h);
   };
   {
@@ -927,7 +920,7 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
 {
   using T = typename Store<S>::C;
   using P = typename PairOf<T>::type;
-  constexpr bool RR = Store<S>::DEV && WRITE_U && WRITE_V;
+  constexpr bool RR = Store<S>::DEV;  // the residual box of the landed u box
   using G = Geo<S, READ_V, RR, W>;
   constexpr int BW = Strip<W>::BW;
   const int tx = threadIdx.x;
@@ -947,7 +940,6 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
   } else {
     const int ib = ts.i0 + CH * ts.b, j = ts.j0 + tx;
     const S *sv = sbox + G::V_OFF / sizeof(S);
-    const S *sr = sbox + G::R_OFF / sizeof(S);
     // 16-bit storage: the scales of the output rows' tile, loaded once per chunk and again at
     // the row where the chunk crosses into the next tile row (CTA-uniform)
     float4 scv = make_float4(0.f, 0.f, 0.f, 0.f), ivv = scv;
@@ -960,23 +952,21 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
     }
 #define FG2_ROW(R)                                                                                         \
   {                                                                                                        \
-    P vrow[NP], rrow[NP];                                                                                  \
+    P vrow[NP];                                                                                            \
     if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);                                 \
-    if (RR) load_cell<S>(sr + (R * G::VBW + tx + G::VOFF) * NV, rrow);                                     \
     if (Store<S>::DEV && WRITE_U && ib + R == next_tile_row) {                                             \
       scv = __ldg(ts.gr.scale + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);                              \
       ivv = __ldg(ts.gr.inv + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);                                \
     }                                                                                                      \
     lead_row<T, M2, R, BW * NV>(base, a, st);                                                              \
-    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, rrow, ib + R, j, ts.iend, scv, ivv, a, ts.gr, \
+    emit_row<S, M2, R, READ_V, WRITE_V, WRITE_U, CFL, SC>(vrow, ib + R, j, ts.iend, scv, ivv, a, ts.gr,       \
                                                           st, ts.whole, ts.rim, nan, rate, ts.cg);         \
   }
     if constexpr (rolled_rows()) {
 #pragma unroll 1
       for (int R = 0; R < CH; ++R) {
-        P vrow[NP], rrow[NP];
+        P vrow[NP];
         if (READ_V) load_cell<S>(sv + (R * G::VBW + tx + G::VOFF) * NV, vrow);
-        if (RR) load_cell<S>(sr + (R * G::VBW + tx + G::VOFF) * NV, rrow);
         if (Store<S>::DEV && WRITE_U && ib + R == next_tile_row) {
           scv = __ldg(ts.gr.scale + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);
           ivv = __ldg(ts.gr.inv + (next_tile_row >> 6) * ts.gr.tiles2 + ts.tj);
@@ -992,7 +982,7 @@ __device__ __forceinline__ void stencil_chunk(const typename Store<S>::C *base, 
           FG2_FRONT(0) FG2_FRONT(1) FG2_FRONT(2) FG2_FRONT(3) FG2_FRONT(4) FG2_FRONT(5) FG2_FRONT(6)
 #undef FG2_FRONT
         }
-        finish_row<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC>(cell, qc, vrow, rrow, ib + R, j, ts.iend, scv, ivv, a,
+        finish_row<S, M2, READ_V, WRITE_V, WRITE_U, CFL, SC>(cell, qc, vrow, ib + R, j, ts.iend, scv, ivv, a,
                                                              ts.gr, ts.whole, ts.rim, nan, rate, ts.cg);
       }
     } else {
@@ -1026,7 +1016,7 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
 {
   using T = typename Store<S>::C;
   constexpr bool DEV = Store<S>::DEV;
-  constexpr bool RR = DEV && WRITE_U && WRITE_V;  // the stage reads the rounding residual
+  constexpr bool RR = DEV;  // 16-bit storage: the residual of every u box is loaded too
   using G = Geo<S, READ_V, RR, W>;
   constexpr int BW = Strip<W>::BW, NT = Strip<W>::NT;
   constexpr int NS = G::NSLOT;
@@ -1100,7 +1090,7 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
     bool live = false;
     if (__all_sync(FULL, landed)) {
       live = advance(0);
-      if (live) decode_box<S, BW, NT>(slot(0), dec, tx, box_row(), ts.j0, ts.gr);
+      if (live) decode_box<S, BW, NT>(slot(0), slot(0) + G::R_OFF / sizeof(S), dec, tx, box_row(), ts.j0, ts.gr);
     }
     failed = __syncthreads_or(!landed);
     for (int n = 0; live && !failed; ++n) {
@@ -1111,7 +1101,8 @@ __global__ void __launch_bounds__(W, min_blocks<S, W>()) substage_kernel(const G
       if (__all_sync(FULL, landed)) {
         live = advance(n + 1);
         if (live)
-          decode_box<S, BW, NT>(slot(n + 1), dec + (size_t)((n + 1) & 1) * (G::DEC_ONE / sizeof(float)), tx, box_row(),
+          decode_box<S, BW, NT>(slot(n + 1), slot(n + 1) + G::R_OFF / sizeof(S),
+                                dec + (size_t)((n + 1) & 1) * (G::DEC_ONE / sizeof(float)), tx, box_row(),
                                 ts.j0, ts.gr);
       }
       failed = __syncthreads_or(!landed);

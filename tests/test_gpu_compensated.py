@@ -1,20 +1,21 @@
 """Compensated 16-bit deviation storage (storage f16 / bf16).
 
 The state is held as the 16-bit number S (value bg + s h) less its rounding residual e,
-which the library keeps in a second 16-bit array (stage 1's residual rides in the RK3
-register v instead), so every rounding of the state is compensated (two-sum) and the state
-itself is tracked to about 2^-23 (FP16) or 2^-17 (BF16) of its tile scale.  What remains is
-the stencil: it reads S, so the right-hand side sees the rounding of the 16-bit numbers.
+which the library keeps beside it in a second 16-bit array (one per ping-pong parity of the
+state, written by every stage that writes the state), so every rounding of the state is
+compensated (two-sum) and the state itself is tracked to about 2^-23 (FP16) or 2^-17 (BF16)
+of its tile scale.  The stencil reads that compensated state, T = S - e, decoded from both
+arrays, not the 16-bit numbers.
 
 * Upload/download: the state comes back to within the residual's own rounding.
 * Small increments: with a step that changes the state by less than half a 16-bit unit, the
   compensated state moves with the FP32 one (an uncompensated store would not move at all),
   to a small fraction of a unit after 20 steps.
-* Accuracy against FP64 (Kelvin-Helmholtz layer, 256^2, 100 steps): the density error stays
-  within 1.5x of the floor of any scheme whose stencil reads the 16-bit numbers -- an FP64 CPU
-  run that keeps the state exact and evaluates the right-hand side on the coded state
-  (tests/helpers.py stencil_on_codes, on the oracle port) -- and the ratio to the FP32 error
-  is printed."""
+* Accuracy against FP64 (Kelvin-Helmholtz layer, 256^2, 100 steps): FP16 storage keeps the
+  density error within 2x of the FP32 path's; BF16 (8 + 8 significant bits) well below the
+  floor of any scheme whose stencil reads the 16-bit numbers (an FP64 CPU run that keeps the
+  state exact and evaluates the right-hand side on the coded state, tests/helpers.py
+  stencil_on_codes on the oracle port)."""
 import numpy as np
 import pytest
 
@@ -78,7 +79,7 @@ def test_increments_below_half_a_unit_accumulate(storage, dt, cuda):
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
-def test_density_error_at_the_stencil_on_codes_floor(storage, cuda):
+def test_density_error_against_fp64(storage, cuda):
     n, steps = 256, 100
     x0 = fg2_b200.setup_evaluate("kh", n, n, seed=2)[0]
     d1, d2 = reference_delta(n, n, 1.0, 1.0)
@@ -91,7 +92,10 @@ def test_density_error_at_the_stencil_on_codes_floor(storage, cuda):
     o = Oracle("hydro", "f64", "port")
     o.set_delta(d1, d2)
     floor = rho_rel_l2(stencil_on_codes(o, x0, steps, dt, storage), ref)
-    print(f"{storage}: density rel L2 vs FP64 {e16:.3e} = {e16 / e32:.0f}x FP32 ({e32:.3e}); "
+    print(f"{storage}: density rel L2 vs FP64 {e16:.3e} = {e16 / e32:.2f}x FP32 ({e32:.3e}); "
           f"stencil-on-codes floor {floor:.3e}")
     assert e32 < floor
-    assert e16 <= 1.5 * floor, (e16, floor)
+    if storage == "f16":
+        assert e16 <= 2.0 * e32, (e16, e32)  # the mixed-precision accuracy bar
+    else:
+        assert e16 <= 0.25 * floor, (e16, floor)
