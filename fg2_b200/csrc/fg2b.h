@@ -119,9 +119,10 @@ enum ErrorBits : unsigned { ERR_TMA_TIMEOUT = 1u, ERR_QUEUE_TIMEOUT = 2u };
 constexpr int SCALE_TILE = 64;
 //
 // The state is kept exactly as S - e, S the stored number's value and e the rounding error of
-// the encode that produced it (the residual, the low part of a two-sum).  e is stored in the
-// array r (same layout as v, interior cells only) as the 16-bit number e / s * RESID_SCALE:
-// |e| <= s 2^-12 for FP16 numbers |h| <= 1, so the stored residual is at most about 1.
+// the encode that produced it (the residual, the low part of a two-sum).  e is stored in a
+// residual array (layout of u, ghost images included; one per ping-pong parity of u) as the
+// 16-bit number e / s * RESID_SCALE: |e| <= s 2^-12 for FP16 numbers |h| <= 1, so the stored
+// residual is at most about 1.
 constexpr int DEV_MAX_FIELDS = 4;  // the codes hold one background and scale per field
 constexpr double RESID_SCALE = 4096.0;
 struct DevCode {

@@ -42,12 +42,14 @@
 // the window never moves.
 //
 // Deviation storage.  With FP16 / BF16 state arrays (S = __half / __nv_bfloat16) the stencil
-// still runs in FP32: when a u chunk lands, the CTA decodes it (bg + s h, s of the cell's
-// 64 x 64 tile) into an FP32 copy in shared memory that the stencil reads; v is converted on
-// load; u' is encoded with its tile's 1/s and v stored as 16-bit numbers.  The rounding
-// residual e = encode(u') - u' of a stage that has a successor is carried into that stage
-// through v: v is stored as v - e / (beta' gamma' dt), so the next update u'' = u'(stored) +
-// gamma' dt (F + beta' v) subtracts e again (src/step.cpp:24-35 unchanged otherwise).
+// still runs in FP32.  The state is the 16-bit number less its rounding residual e, which a
+// second 16-bit array (one per ping-pong parity of u) holds as e / s * RESID_SCALE: each u box
+// lands with the residual box of the same cells, and the CTA decodes both into the state
+// T = bg + s h - s e' / RESID_SCALE (s of the cell's 64 x 64 tile) in an FP32 copy in shared
+// memory that the stencil reads.  v is converted on load; u' = T + gamma dt v is encoded with
+// its tile's 1/s, its residual e' = encode(u') - u' stored beside it, and v stored as 16-bit
+// numbers, so every rounding of the state is compensated (src/step.cpp:24-35 unchanged
+// otherwise).
 //
 // Stencil weights.  A single-grid launch folds 1/Delta into the weights (constant-bank
 // operands).  A batch launch (SC) uses the reference's plain weights and multiplies each
