@@ -505,7 +505,7 @@ int fg2_batch_autotune(fg2_batch *b, int reps, double *best_ms)
       for (int warps : {0, 4, 8, 12})
         cands.push_back({strip, nb, warps * 32 / strip, std::numeric_limits<double>::infinity()});
   const int keep_nb = b->nb, keep_ctas = b->max_ctas, keep_strip = b->strip;
-  // 16-bit storage: a step of dt = 0 re-encodes the state and drops its rounding residual, so
+  // 16-bit storage: a step of dt = 0 re-encodes the state and its rounding residual, so
   // the members' arrays are kept aside and put back afterwards
   void *keep = nullptr;
   if (b->members[0]->dev_storage) {

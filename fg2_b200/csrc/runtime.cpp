@@ -611,7 +611,7 @@ int fg2_sim_autotune(fg2_sim *s, int reps, double *best_ms)
           cands.push_back({nb, warps * 32 / STRIP_DEFAULT, tail, 0.0});
   const int keep_nb = s->nb, keep_ctas = s->max_ctas, keep_tail = s->tail, keep_cur = s->cur;
   const bool keep_ghosts = s->ghosts_valid, keep_smax = s->smax_valid;
-  // 16-bit storage: a step of dt = 0 re-encodes the state and drops its rounding residual, so
+  // 16-bit storage: a step of dt = 0 re-encodes the state and its rounding residual, so
   // the state and the residual are kept aside and put back afterwards
   const size_t bytes = array_elems(s) * elem_size(s->storage);
   void *keep = nullptr;
