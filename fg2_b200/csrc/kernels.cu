@@ -77,6 +77,18 @@ struct Store<__nv_bfloat16> {
   static __device__ __forceinline__ __nv_bfloat162 from2(float2 x) { return __float22bfloat162_rn(x); }
 };
 
+// Type of the rounding residual of a 16-bit state: FP16 for both storages (a BF16 state's
+// residual e / s * RESID_SCALE is at most about 8, which FP16 holds to 11 bits where BF16
+// would keep 8).
+template <class S>
+struct Resid {
+  using type = S;
+};
+template <>
+struct Resid<__nv_bfloat16> {
+  using type = __half;
+};
+
 // Parameters of one substage launch, rounded to the storage precision T: the stencil
 // weights both as scalars and broadcast to both lanes of a pair (so packed instructions read
 // them straight from the constant bank), the scheme's parameters as scalars.
@@ -274,7 +286,7 @@ CUresult make_grid_desc(GridDesc *d, const void *u_in, void *u_out, void *v, con
   r = encode_map(&d->tm_v, v, L, storage, vbw, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
   if (r != CUDA_SUCCESS) return r;
   if (dev && dev->r) {  // the input's rounding residual, in boxes like u's (halo included)
-    r = encode_map(&d->tm_r, dev->r, L, storage, sw + 2 * GL, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
+    r = encode_map(&d->tm_r, dev->r, L, resid_storage(storage), sw + 2 * GL, sub::CH, L.n2 + 2 * GL, L.n1 + 2 * GT);
     if (r != CUDA_SUCCESS) return r;
   } else {
     d->tm_r = d->tm_v;  // never read: only 16-bit stages load r
@@ -506,7 +518,8 @@ __device__ __forceinline__ double value_at(const S *u, const Layout &L, const De
     const float sf = f == 0 ? sc.x : f == 1 ? sc.y : f == 2 ? sc.z : sc.w;
     const double x = (double)fmaf(sf, Store<S>::to(u[L.at(f, i, j)]), dc.bg[f]);
     if (!dc.r) return x;
-    const double e = (double)Store<S>::to(reinterpret_cast<const S *>(dc.r)[L.at(f, i, j)]) * (double)sf / RESID_SCALE;
+    using R = typename Resid<S>::type;
+    const double e = (double)Store<R>::to(reinterpret_cast<const R *>(dc.r)[L.at(f, i, j)]) * (double)sf / RESID_SCALE;
     return x - e;
   }
 }
@@ -623,7 +636,8 @@ __global__ void encode_kernel(S *u, const float *src, const Layout L, const DevC
     // the rounding residual e = S - x, kept as e / s * RESID_SCALE (the substage's encoding)
     if (dc.r) {
       const float e = fmaf(sf, Store<S>::to(h), dc.bg[f]) - src[k];
-      reinterpret_cast<S *>(dc.r)[L.at(f, i, j)] = Store<S>::from(e * (inv * (float)RESID_SCALE));
+      using R = typename Resid<S>::type;
+      reinterpret_cast<R *>(dc.r)[L.at(f, i, j)] = Store<R>::from(e * (inv * (float)RESID_SCALE));
     }
   }
 }

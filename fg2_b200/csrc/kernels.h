@@ -78,6 +78,8 @@ int strip_width(int strip);
 // Tiles of one grid for a tile height of nb blocks of 7 rows, a strip width and a number of
 // one-block tail bands (0: defaults, no tail bands).
 int substage_tiles(const Layout &L, int nb = 0, int strip = 0, int tail = 0);
+// Storage type of the rounding residual of a 16-bit state (FP16 for BF16 states too).
+inline int resid_storage(int storage) { return storage == ST_BF16 ? ST_F16 : storage; }
 // The row bands of a grid of n1 rows in the fused kernel's processing order (reverse: a
 // reverse launch's), as (i0, iend, blocks) triples into out[3 cap]; returns the band count.
 int tile_bands(int n1, int nb, int tail, int reverse, int *out, int cap);

@@ -180,7 +180,7 @@ int do_bcond(fg2_sim *s)
 {
   CK(launch_bcond(s->storage, s->u[s->cur], s->L, s->p1, s->p2, s->stream));
   // 16-bit storage: the residual's ghost cells image the same cells (the stencil reads T = S - e)
-  if (s->dev_storage) CK(launch_bcond(s->storage, s->r[s->cur], s->L, s->p1, s->p2, s->stream));
+  if (s->dev_storage) CK(launch_bcond(resid_storage(s->storage), s->r[s->cur], s->L, s->p1, s->p2, s->stream));
   s->ghosts_valid = true;
   return FG2_OK;
 }

@@ -637,7 +637,9 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
     if (WRITE_U) store_cell<S>(gr.u_out + o, qp);
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
-  RawCell<S> raw, rraw;
+  using RS = typename Resid<S>::type;
+  RawCell<S> raw;
+  RawCell<RS> rraw;
   if constexpr (DEV) {
     if (WRITE_U) {
       // encode u' with its tile's 1/s; e' = S' - u' is the rounding residual, stored as
@@ -651,7 +653,7 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
         e[p] = fmac(sc[p], hs[p], gr.bg[p]) - qp[p];
         ro[p] = e[p] * (iv[p] * lit<P>(RESID_SCALE));
       }
-      encode_cell<S>(gr.r + o, ro, unused, rraw.v);
+      encode_cell<RS>(reinterpret_cast<RS *>(gr.r) + o, ro, unused, rraw.v);
     }
     if (WRITE_V) store_cell<S>(gr.v + o, vn);
   }
@@ -671,7 +673,7 @@ __device__ __forceinline__ void finish_row(const Cell<typename Store<S>::C, NV> 
       }
       else {
         rim_images_raw<S>(gr.u_out, gr.L, i, j, raw, gr.p1, gr.p2);
-        rim_images_raw<S>(gr.r, gr.L, i, j, rraw, gr.p1, gr.p2);
+        rim_images_raw<RS>(reinterpret_cast<RS *>(gr.r), gr.L, i, j, rraw, gr.p1, gr.p2);
       }
     }
     if (CFL) rate = fmax(rate, cfl_rate<T>(qn, a.p, gr.inv1, gr.inv2, i, j, dl1, dl2, cg));
@@ -819,6 +821,7 @@ template <class S, int BOXW, int NT>
 __device__ __forceinline__ void decode_box(const S *box, const S *rbox, float *dec, int tx, int prow0, int j0,
                                            const GridRegs<S> &gr)
 {
+  using R = typename Resid<S>::type;
   constexpr int EXTRA = BOXW - NT;  // columns beyond one per thread
   const int n1 = gr.L.n1, n2 = gr.L.n2;
   const int i0 = prow0 - GT;
@@ -832,7 +835,7 @@ __device__ __forceinline__ void decode_box(const S *box, const S *rbox, float *d
     const float2 scp[2] = {make_float2(sc.x, sc.y), make_float2(sc.z, sc.w)};
     float2 h[NP], e[NP];
     load_cell<S>(box + (r * BOXW + c) * NV, h);
-    load_cell<S>(rbox + (r * BOXW + c) * NV, e);
+    load_cell<R>(reinterpret_cast<const R *>(rbox) + (r * BOXW + c) * NV, e);
 #pragma unroll
     for (int p = 0; p < NP; ++p) h[p] = fmac(scp[p] * lit<float2>(-1.0 / RESID_SCALE), e[p], fmac(scp[p], h[p], gr.bg[p]));
     st_cell<float>(dec + (r * BOXW + c) * NV, h);

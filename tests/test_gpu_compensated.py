@@ -3,8 +3,8 @@
 The state is held as the 16-bit number S (value bg + s h) less its rounding residual e,
 which the library keeps beside it in a second 16-bit array (one per ping-pong parity of the
 state, written by every stage that writes the state), so every rounding of the state is
-compensated (two-sum) and the state itself is tracked to about 2^-23 (FP16) or 2^-17 (BF16)
-of its tile scale.  The stencil reads that compensated state, T = S - e, decoded from both
+compensated (two-sum) and the state itself is tracked to about 2^-23 (FP16) or 2^-20 (BF16)
+of its tile scale (the residual is an FP16 number for both).  The stencil reads that compensated state, T = S - e, decoded from both
 arrays, not the 16-bit numbers.
 
 * Upload/download: the state comes back to within the residual's own rounding.
@@ -26,8 +26,8 @@ from oracle.oracle import Oracle, reference_delta
 pytestmark = pytest.mark.gpu
 
 UNIT = {"f16": 2.0 ** -11, "bf16": 2.0 ** -8}
-# the residual is itself a 16-bit number (11 or 8 significant bits) of |e| <= s unit / 2
-RESID = {"f16": 2.0 ** -22, "bf16": 2.0 ** -16}
+# the residual is itself an FP16 number (11 significant bits) of e / s * 4096, |e| <= s unit / 2
+RESID = {"f16": 2.0 ** -22, "bf16": 2.0 ** -19}
 
 
 def run(storage, x0, steps, dt, n1, n2):
