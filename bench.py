@@ -881,7 +881,7 @@ def run_fused(args):
     dist = dist_init(world, "nccl")
 
     sim = fg2_b200.Sim(N1, N2, scheme=SCHEME, storage=args.storage)
-    b_alg = B_ALG_F16 if args.storage in ("f16", "bf16") else B_ALG  # 160 B FP32, 112 B 16-bit
+    b_alg = B_ALG_F16 if args.storage in ("f16", "bf16") else B_ALG  # 160 B FP32, 128 B 16-bit
     fpc = flop_model(NVAR, sim.lib.fg2_eqns_flop())  # 891 for hydro
     sim.config()
     state = initial_state()
