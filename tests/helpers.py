@@ -97,3 +97,35 @@ def stencil_on_codes(oracle, x0, steps, dt, storage, p1=1, p2=1):
             oracle.kick(vp, up, 0.0, beta[k])
             T = T + gamma[k] * dt * vp[inner]
     return T
+
+
+def compensated_stencil(oracle, x0, steps, dt, storage, p1=1, p2=1):
+    """The library's compensated 16-bit scheme, emulated with FP64 arithmetic: each state is
+    stored as the 16-bit number S = bg + s round16((u - bg) / s) and its residual as the FP16
+    number r = (S - u) / s * 4096; every substage's stencil reads T = S - s r / 4096, v is
+    stored as plain 16-bit numbers between substages.  Returns T after `steps` RK3 steps."""
+    from oracle.oracle import HALO
+    beta = [0.0, -5.0 / 9.0, -153.0 / 128.0]
+    gamma = [1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0]
+    bg, s = deviation_codes(x0)
+    n1, n2, _ = x0.shape
+
+    def store(u):  # (S, T) of a state u
+        S = bg + s * round16((u - bg) / s, storage)
+        r = round16((S - u) / s * 4096.0, "f16")
+        return S - s * r / 4096.0
+
+    T = store(np.asarray(x0, np.float64))
+    up = oracle.padded(T)
+    vp = oracle.padded(np.zeros_like(T))
+    inner = (slice(HALO, HALO + n1), slice(HALO, HALO + n2))
+    for _ in range(steps):
+        for k in range(3):
+            up[inner] = T
+            oracle.bcond(up, p1, p2)
+            oracle.kick(vp, up, 0.0, beta[k])
+            v = vp[inner].copy()
+            T = store(T + gamma[k] * dt * v)
+            if k < 2:
+                vp[inner] = round16(v, storage)
+    return T
