@@ -44,9 +44,9 @@
 // Deviation storage.  With FP16 / BF16 state arrays (S = __half / __nv_bfloat16) the stencil
 // still runs in FP32.  The state is the 16-bit number less its rounding residual e, which a
 // second 16-bit array (one per ping-pong parity of u) holds as e / s * RESID_SCALE: each u box
-// lands with the residual box of the same cells, and the CTA decodes both into the state
-// T = bg + s h - s e' / RESID_SCALE (s of the cell's 64 x 64 tile) in an FP32 copy in shared
-// memory that the stencil reads.  v is converted on load; u' = T + gamma dt v is encoded with
+// lands with the residual box of the same cells (residual numbers r), and the CTA decodes
+// both into the state T = bg + s h - s r / RESID_SCALE (s of the cell's 64 x 64 tile) in an
+// FP32 copy in shared memory that the stencil reads.  v is converted on load; u' = T + gamma dt v is encoded with
 // its tile's 1/s, its residual e' = encode(u') - u' stored beside it, and v stored as 16-bit
 // numbers, so every rounding of the state is compensated (src/step.cpp:24-35 unchanged
 // otherwise).
@@ -813,8 +813,9 @@ __device__ __forceinline__ void load_grid(const GridDesc &gd, const KParams<type
 // Deviation storage: decodes the landed 7-row u box (padded rows prow0 .., box column 0 =
 // padded column j0) and its residual box into FP32 cells dec ([row][BOXW][NV]): the state
 // T = bg + s h - s r / RESID_SCALE, s of the tile of the interior cell each value images, so
-// the stencil reads the state with its rounding compensated, not the 16-bit numbers.  Thread t decodes column t of every row and, for t below
-// 7 (BOXW - NT), one cell of the columns beyond the strip, so the work is even across warps.
+// the stencil reads the state with its rounding compensated, not the 16-bit numbers.  Thread
+// t decodes column t of every row and, for t below 7 (BOXW - NT), one cell of the columns
+// beyond the strip, so the work is even across warps.
 // A chunk whose 7 rows lie in one tile row (all but about one chunk in nine) reads each
 // column's scales once.
 template <class S, int BOXW, int NT>
